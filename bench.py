@@ -1,0 +1,420 @@
+#!/usr/bin/env python
+"""Benchmark of the LTE turbo decoder on B200.
+
+Workload (one "step" = one decode call over one batch resident in HBM): K=6144 code blocks
+(QPP f1=263, f2=480), rate 1/3 with 12 tail bits, 4096 code blocks per call, exact Log-MAP,
+8 full iterations, no early stop, FP32 channel LLRs 2y/sigma^2 of seeded uniform info bits
+over BPSK/AWGN; the 7 Eb/N0 points 0.0..1.2 dB (step 0.2) each get their own batch and the
+steps cycle through them.  Metric: decoded information Mbit/s (K bits per code block).
+
+Lines printed by rank 0 (one JSON object):
+  value     -- device-resident decode throughput, CUDA events on the launching stream,
+               max over ranks, whole-job aggregate (weak scaling: every rank decodes its own
+               batches, code blocks are independent, no collective on the data path)
+  e2e       -- the same metric through the C ABI with pinned host buffers: H2D of the LLRs,
+               decode, D2H of posterior/flags inside the timed region (tc_decode, TC_MEM_HOST)
+  roofline  -- dominant kernel (SISO half-iteration) against the SFU (MUFU) issue roofline
+  roofline_hbm -- the same kernel's algorithmic bytes against measured HBM bandwidth
+  cpu_baseline -- the reference CPU decoder (oracle/_ref) on all host cores, bounded sample
+  ber_bler  -- BER/BLER per Eb/N0 point of the GPU decode (and of the CPU sample)
+
+`--impl reference` times the reference's own CPU decoder instead, on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "info Mbit/s @8 iters, matched BLER: batched vs plain GPU vs CPU ref; adjoint err"
+EBN0 = [0.0, 0.2, 0.4, 0.6, 0.8, 1.0, 1.2]
+K = 6144
+# SURVEY-d algorithmic work of one trellis step of one SISO: 30 max*, 2 transcendentals each
+TRANSC_PER_STEP = 60
+# algorithmic HBM bytes per info bit of a whole decode: 3(K+4) LLRs in + K posteriors out
+BYTES_PER_BIT = 4.0 * (3 * (K + 4) + K) / K
+MUFU_PER_SM_CLK = 16  # B200 SFU lanes per SM per clock (4 per SM sub-partition)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=14)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--n-cb", type=int, default=4096)
+    ap.add_argument("--iterations", type=int, default=8)
+    ap.add_argument("--window", type=int, default=0)
+    ap.add_argument("--guard", type=int, default=-1)
+    ap.add_argument("--schedule", choices=["plain", "persistent"], default="plain")
+    ap.add_argument("--points", type=int, default=len(EBN0), help="Eb/N0 points to use")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if args.impl == "b200" else "gloo"
+        if backend == "nccl":
+            import torch
+
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64,
+                     device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(schedule: str):
+    """DRAM bytes per trellis step of the SISO kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "siso_dram_traffic.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)[schedule]["dram_bytes_per_step"])
+    except (OSError, KeyError, ValueError, TypeError):
+        return None
+
+
+# ------------------------------------------------------------------------------------------
+def cpu_reference_sample(tc, seconds: float, threads: int = 0):
+    """The reference decoder (oracle/_ref, else the oracle port) over a bounded sample of the
+    same workload on all host cores.  Returns (Mbit/s, cores, kind, sample description, bits,
+    posterior)."""
+    import oracle
+
+    cores = threads or os.cpu_count() or 1
+    if oracle.reference_available():
+        lib, kind = oracle.Reference(), "reference"
+    else:
+        lib, kind = oracle.Oracle(), "port"
+    # one probe block to size the sample to ~`seconds` of wall time on `cores` threads
+    bits, llr = tc.awgn_code_blocks(77, [K], 0.6)
+    t = time.perf_counter()
+    lib.decode_batch(np.array([K], np.int32), np.zeros(1, np.int32), llr, np.zeros(1, np.int64),
+                     np.zeros(1, np.int64), 8, threads=1)
+    per_cb = time.perf_counter() - t
+    n = int(max(cores, min(cores * 64, seconds * cores / max(per_cb, 1e-3))))
+    n = max(cores, (n // cores) * cores)
+    eb = np.array([EBN0[i % len(EBN0)] for i in range(n)], np.float32)
+    bits, llr = tc.awgn_code_blocks(78, [K] * n, eb)
+    lo = np.arange(n, dtype=np.int64) * 3 * (K + 4)
+    oo = np.arange(n, dtype=np.int64) * K
+    t = time.perf_counter()
+    post, _, _ = lib.decode_batch(np.full(n, K, np.int32), np.zeros(n, np.int32), llr, lo, oo, 8,
+                                  threads=cores)
+    dt = time.perf_counter() - t
+    sample = (f"{n} code blocks of K=6144 (Eb/N0 0.0..1.2 dB cycled), 8 iterations, one block "
+              f"per task on {cores} threads ({kind})")
+    return n * K / dt / 1e6, cores, kind, sample, bits, post, eb
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the reference CPU decoder on the host cores, rank 0 only."""
+    if rank != 0:
+        return
+    import turbo_cpp_b200 as tc
+
+    steps = []
+    cores = os.cpu_count() or 1
+    for i in range(args.warmup + args.steps):
+        mbps, cores, kind, sample, _, _, _ = cpu_reference_sample(
+            tc, max(2.0, args.cpu_seconds / 3), cores)
+        if i >= args.warmup:
+            steps.append(mbps)
+    v = float(np.mean(steps))
+    line = {
+        "metric": METRIC, "value": v, "unit": "Mbit/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": args.n_cb * K / (v * 1e6) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded uniform info bits, BPSK/AWGN, Eb/N0 0.0..1.2 dB, FP32 LLRs",
+        "config": workload_config(args), "impl": "reference",
+        "cpu_baseline": {"value": v, "unit": "Mbit/s", "cores": cores, "kind": kind,
+                         "sample": sample + "; each step one such sample"},
+        "e2e": {"value": v, "unit": "Mbit/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args):
+    return {
+        "workload": "LTE turbo decode: K=6144 (QPP f1=263 f2=480), rate 1/3 + 12 tail bits, "
+                    f"{args.n_cb} code blocks per call, exact Log-MAP, {args.iterations} "
+                    "iterations, no early stop, Eb/N0 0.0..1.2 dB step 0.2",
+        "n_cb": args.n_cb, "k": K, "iterations": args.iterations,
+        "window": args.window or 128, "guard": 64 if args.guard < 0 else args.guard,
+        "schedule": args.schedule, "ebn0_db": EBN0[:args.points],
+        "l2": "inputs 302 MB per step > 126 MB L2 (no flush needed)",
+    }
+
+
+def ber_bler(post, bits, n, k):
+    e = ((post >= 0) != bits).reshape(n, k)
+    return float(e.mean()), float(e.any(1).mean())
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        barrier(world)
+        return
+    import torch
+
+    import turbo_cpp_b200 as tc
+
+    torch.cuda.set_device(local)
+    dev = tc.Decoder(local)
+    n, it = args.n_cb, args.iterations
+    opts = tc.DecodeOptions(it, False, args.window, args.guard,
+                            tc.SCHEDULE_PERSISTENT if args.schedule == "persistent"
+                            else tc.SCHEDULE_PLAIN)
+    cbs, llr_len, post_len = tc.Decoder.layout([K] * n)
+    points = EBN0[:args.points]
+    batches, truth = [], []
+    for j, eb in enumerate(points):
+        bits, llr = tc.awgn_code_blocks(1000 * rank + j, [K] * n, eb)
+        batches.append(torch.from_numpy(llr).to(f"cuda:{local}"))
+        truth.append(bits)
+    post = torch.empty(post_len, dtype=torch.float32, device=f"cuda:{local}")
+    stream = torch.cuda.current_stream()
+
+    def step(i):
+        x = batches[i % len(batches)]
+        dev.decode_device(cbs, n, x.data_ptr(), llr_len, post.data_ptr(), post_len,
+                          options=opts, stream=stream.cuda_stream)
+
+    # BER/BLER per point (outside the timed region)
+    quality = []
+    for j in range(len(points)):
+        step(j)
+        stream.synchronize()
+        ber, bler = ber_bler(post.cpu().numpy(), truth[j], n, K)
+        quality.append({"ebn0_db": points[j], "ber": ber, "bler": bler, "blocks": n})
+
+    for i in range(args.warmup):
+        step(i)
+    stream.synchronize()
+    dev.timing(reset=True)
+    dev.set_timing(True)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        t0.record(stream)
+        for i in range(args.steps):
+            step(i)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    dev.set_timing(False)
+    tm = dev.timing(reset=True)
+    ms = max_over_ranks(t0.elapsed_time(t1), world)
+    bits_total = world * n * K * args.steps
+    value = bits_total / (ms / 1e3) / 1e6
+    clocks = clk.summary()
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        host_llr = [torch.empty(llr_len, dtype=torch.float32).pin_memory() for _ in points]
+        for j, b in enumerate(batches):
+            host_llr[j].copy_(b)
+        host_post = torch.empty(post_len, dtype=torch.float32).pin_memory()
+        host_ok = torch.empty(n, dtype=torch.uint8).pin_memory()
+        host_it = torch.empty(n, dtype=torch.int32).pin_memory()
+        import ctypes
+
+        host_opt, _keep = dev._opts(opts, tc.MEM_HOST)
+
+        def host_step(i):
+            x = host_llr[i % len(host_llr)]
+            tc._call("tc_decode", dev._h, n, ctypes.addressof(cbs), llr_len, x.data_ptr(),
+                     post_len, host_post.data_ptr(), host_ok.data_ptr(), host_it.data_ptr(),
+                     ctypes.addressof(host_opt))
+        for i in range(args.warmup):
+            host_step(i)
+        barrier(world)
+        t = time.perf_counter()
+        for i in range(args.steps):
+            host_step(i)
+        e2e_s = max_over_ranks(time.perf_counter() - t, world)
+        e2e = {"value": bits_total / e2e_s / 1e6, "unit": "Mbit/s",
+               "h2d_bytes_per_step": llr_len * 4, "d2h_bytes_per_step": post_len * 4 + n * 5,
+               "timing": "wall clock around synchronous tc_decode calls, max over ranks"}
+
+    # ---- roofline of the dominant kernel (SISO launch), from the live CUDA-event timings ----
+    props = torch.cuda.get_device_properties(local)
+    sm_mhz = clocks["sm_mhz"] or 1965.0
+    avg_launch_ms = tm["siso_ms"] / max(tm["siso_launches"], 1)
+    steps_per_launch = tm["trellis_steps"] / max(tm["siso_launches"], 1)
+    achieved = TRANSC_PER_STEP * steps_per_launch / (avg_launch_ms / 1e3) / 1e9
+    peak = props.multi_processor_count * MUFU_PER_SM_CLK * sm_mhz * 1e6 / 1e9
+    traffic_per_step = ncu_traffic(args.schedule)
+    hbm_peak, hbm_src = measured_peaks()
+    alg_bytes_launch = steps_per_launch * BYTES_PER_BIT / 2 / it  # share of one decode's bytes
+    hbm_achieved = alg_bytes_launch / (avg_launch_ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mbit/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded uniform info bits, BPSK/AWGN at Eb/N0 0.0..1.2 dB (one batch "
+                "per point, steps cycle through them), FP32 LLRs 2y/sigma^2",
+        "config": workload_config(args),
+        "roofline": {
+            "bound": "sfu", "achieved": achieved, "peak": peak, "unit": "Gtransc/s",
+            "frac": achieved / peak, "traffic": None if traffic_per_step is None
+            else traffic_per_step * steps_per_launch,
+            "kernel": "siso_plain_kernel (one SISO half-iteration over all code blocks)",
+            "work": f"{TRANSC_PER_STEP} transcendentals per trellis step (30 exact max*), "
+                    f"{steps_per_launch:.0f} steps per launch",
+            "avg_launch_ms": avg_launch_ms,
+            "peak_source": f"{props.multi_processor_count} SMs x {MUFU_PER_SM_CLK} MUFU/clk x "
+                           f"median sampled SM clock {sm_mhz:.0f} MHz (nominal issue rate)",
+        },
+        "roofline_hbm": {
+            "bound": "hbm", "achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
+            "frac": hbm_achieved / hbm_peak, "peak_source": f"{hbm_src} MEASURED_PEAKS hbm_gbs",
+            "work": "16.0 B per info bit per decode (3(K+4) LLRs in, K posteriors out), split "
+                    "over the 2*iterations SISO launches",
+        },
+        "gpu_launches": int(tm["launches"]),
+        "clocks": clocks,
+        "ber_bler": quality,
+    }
+    if e2e:
+        line["e2e"] = e2e
+    # ---- plain per-block GPU path: one code block per call, as the reference API decodes ----
+    per_block = []
+    sub = batches[3 % len(batches)].cpu().numpy()[:8 * 3 * (K + 4)]
+    for r in range(2):
+        t = time.perf_counter()
+        for c in range(8):
+            dev.decode([K], sub[c * 3 * (K + 4):(c + 1) * 3 * (K + 4)], options=opts)
+        if r:
+            per_block.append(8 * K / (time.perf_counter() - t) / 1e6)
+    line["plain_per_block"] = {"value": float(np.mean(per_block)), "unit": "Mbit/s",
+                               "how": "turbo_decode_code_block_gpu semantics: one K=6144 block "
+                                      "per synchronous call, host buffers, 8 blocks"}
+    line["batched_vs_plain_per_block"] = value / line["plain_per_block"]["value"]
+    if rank == 0 and not args.no_cpu:
+        mbps, cores, kind, sample, cbits, cpost, ceb = cpu_reference_sample(tc, args.cpu_seconds)
+        cn = cbits.size // K
+        line["cpu_baseline"] = {"value": mbps, "unit": "Mbit/s", "cores": cores, "kind": kind,
+                                "sample": sample}
+        line["cpu_ber_bler"] = [
+            {"ebn0_db": float(e), "blocks": int((ceb == e).sum()),
+             "ber": float(((cpost >= 0) != cbits).reshape(cn, K)[ceb == e].mean()),
+             "bler": float(((cpost >= 0) != cbits).reshape(cn, K)[ceb == e].any(1).mean())}
+            for e in points]
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    dev.close()
+    barrier(world)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,150 @@
+/*
+ * turbo_b200.h -- C ABI of libturbo_b200.so, the B200 (sm_100a) LTE turbo decoder.
+ *
+ * Every function returns a tc_status (0 = TC_OK), never throws, and leaves a human-readable
+ * detail of the last failure in tc_last_error() (per calling thread).  No CUDA or C++ types
+ * appear here: device pointers, host pointers and streams are plain pointers.
+ *
+ * Each entry point names the Wiseung/Turbo_CPP interface it replaces
+ * (include/turbo_cpp/lte_turbo.h and src/lte_turbo.cpp in that project).
+ */
+#ifndef TURBO_B200_H
+#define TURBO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define TC_API __attribute__((visibility("default")))
+#else
+#define TC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  TC_OK = 0,
+  TC_ERR_INVALID_ARGUMENT = 1, /* reference: std::invalid_argument (sizes, descriptors)       */
+  TC_ERR_OUT_OF_RANGE = 2,     /* reference: std::out_of_range (K not an LTE block size)     */
+  TC_ERR_RUNTIME = 3,          /* reference: std::runtime_error (e.g. K+/K- selection)        */
+  TC_ERR_CUDA = 4,             /* a CUDA runtime call failed                                  */
+  TC_ERR_NO_DEVICE = 5,        /* no CUDA device visible                                      */
+  TC_ERR_TIMEOUT = 6,          /* a bounded device-side wait gave up                          */
+  TC_ERR_CAPACITY = 7          /* request exceeds a fixed capacity                            */
+} tc_status;
+
+TC_API const char* tc_status_name(int status);
+TC_API const char* tc_last_error(void);
+TC_API int tc_version(void); /* major*10000 + minor*100 + patch */
+
+/* ---------------- QPP interleaver ----------------
+ * replaces qpp_interleaver_table / qpp_entry_for_k / qpp_permutation /
+ * qpp_inverse_permutation (lte_turbo.h:94-95, 108-109; lte_turbo.cpp:498-506, 606-622) */
+TC_API int tc_qpp_table_size(void);
+TC_API int tc_qpp_entry(int index, int32_t* k, int32_t* f1, int32_t* f2);
+TC_API int tc_qpp_index(int32_t k, int32_t* index); /* TC_ERR_OUT_OF_RANGE for unsupported K */
+TC_API int tc_qpp_permutation(int32_t k, int32_t* perm /* K */);
+TC_API int tc_qpp_inverse_permutation(int32_t k, int32_t* inv /* K */);
+
+/* ---------------- CRC ----------------
+ * replaces append_crc24a/24b/16/8 and check_crc24a/24b/16/8 (lte_turbo.h:97-104) */
+typedef enum { TC_CRC24A = 0, TC_CRC24B = 1, TC_CRC16 = 2, TC_CRC8 = 3 } tc_crc_kind;
+TC_API int tc_crc_append(int kind, const uint8_t* bits, size_t n, uint8_t* out /* n + L */);
+TC_API int tc_crc_check(int kind, const uint8_t* bits, size_t n, int* ok);
+
+/* ---------------- code-block segmentation ----------------
+ * replaces segment_transport_block (lte_turbo.h:83-92, 106; lte_turbo.cpp:540-604) */
+typedef struct {
+  size_t c, c_plus, c_minus, k_plus, k_minus, filler_bits, l;
+} tc_segmentation;
+/* cb_bits may be NULL (sizes only); otherwise it receives the C blocks back to back,
+ * c_plus*k_plus + c_minus*k_minus bits, and cap is its capacity. */
+TC_API int tc_segment_transport_block(const uint8_t* bits_with_crc, size_t b, tc_segmentation* info,
+                               uint8_t* cb_bits, size_t cap);
+
+/* ---------------- encoder and rate matching ----------------
+ * replace turbo_encode_code_block (lte_turbo.h:111-112), the rate matching inside
+ * encode_transport_block (lte_turbo.cpp:167-278, 690-720) and derate_match_code_block
+ * (lte_turbo.h:116-118).  d012 = [d0 | d1 | d2], each K+4 entries. */
+TC_API int tc_turbo_encode(int32_t k, int32_t filler, const uint8_t* cb_bits, uint8_t* d012);
+TC_API int tc_compute_e(size_t r, size_t g_total, size_t c, uint32_t num_layers, uint32_t mod_order,
+                 size_t* e);
+TC_API int tc_rate_match(int32_t k, int32_t filler, const uint8_t* d012, size_t e, uint32_t rv,
+                  uint8_t* out /* e bits */);
+/* hard bits -> +-8.0 with repetition combining, exactly derate_match_code_block */
+TC_API int tc_derate_match_bits(int32_t k, int32_t filler, const uint8_t* e_bits, size_t e, uint32_t rv,
+                         float* d012_llr);
+/* the same walk over soft channel LLRs (LLR-domain de-rate matching; new) */
+TC_API int tc_derate_match_llr(int32_t k, int32_t filler, const float* e_llr, size_t e, uint32_t rv,
+                        float* d012_llr);
+
+/* ---------------- seeded test channel (new; used by tests and the benchmark) ---------------- */
+TC_API int tc_random_bits(uint64_t seed, uint64_t first, size_t n, uint8_t* bits);
+TC_API int tc_awgn_llr(uint64_t seed, uint64_t first, const uint8_t* bits, size_t n, double sigma2,
+                float* llr);
+
+/* n seeded code blocks: info bits (filler zeros first; last 24 bits CRC24B when crc24b), turbo
+ * encoding, BPSK/AWGN at ebn0_db[i] (rate K/(3(K+4)), LLR = 2y/sigma^2), filler LLRs zeroed.
+ * bits: sum K; llr: 3*sum(K+4), blocks back to back.  threads <= 0: all cores. */
+TC_API int tc_awgn_code_blocks(uint64_t seed, size_t n, const int32_t* k, const int32_t* filler,
+                               const float* ebn0_db, int crc24b, uint8_t* bits, float* llr,
+                               int threads);
+
+/* ---------------- GPU decoder ----------------
+ * replaces turbo_decode_code_block_gpu_stage1 / _stage2 / _stage1_tile8_experimental
+ * (lte_turbo.h:129-155) and their CUDA impls (lte_turbo_cuda.cu:1391-1899): any number of
+ * code blocks of any LTE sizes per call, exact Log-MAP, posterior = Ls + e1 + e2 as
+ * turbo_decode_code_block_cpu (lte_turbo.cpp:736-813). */
+typedef struct tc_decoder tc_decoder;
+TC_API int tc_decoder_create(int device, tc_decoder** out);
+TC_API int tc_decoder_destroy(tc_decoder* dec);
+
+typedef struct {
+  int32_t k;          /* block size: one of the 188 LTE QPP sizes                       */
+  int32_t filler;     /* filler bits at the block start (erasures; zeroed before CRC)   */
+  int64_t llr_offset; /* float offset of [d0|d1|d2] (3*(K+4) floats); multiple of 4       */
+  int64_t out_offset; /* float offset of the block's K posterior LLRs                     */
+} tc_code_block;
+
+enum { TC_MEM_HOST = 0, TC_MEM_DEVICE = 1 };
+enum { TC_SCHEDULE_PLAIN = 0, TC_SCHEDULE_PERSISTENT = 1 };
+
+typedef struct {
+  uint32_t max_iterations; /* default 8                                                   */
+  uint32_t early_stop;     /* stop a block once its hard decisions pass CRC24B            */
+  int32_t window;          /* steps per window; 0 = default (128); >= K = full trellis    */
+  int32_t guard;           /* warm-up steps on each side; < 0 = default (64); multiple of 8 */
+  uint32_t memory;         /* TC_MEM_HOST (synchronous, copies inside) or TC_MEM_DEVICE   */
+  uint32_t schedule;       /* TC_SCHEDULE_PLAIN or TC_SCHEDULE_PERSISTENT                 */
+  const float* scales;     /* host array, 2 per iteration (upper, lower); NULL = 1.0     */
+  void* stream;            /* cudaStream_t for TC_MEM_DEVICE; NULL = the decoder's stream */
+} tc_decode_options;
+
+TC_API int tc_decode_options_init(tc_decode_options* opts);
+
+/* Decodes n_cb code blocks.  llr has llr_len floats, posterior post_len floats; crc_ok
+ * (n_cb bytes) and iterations_used (n_cb words) may be NULL.  With TC_MEM_HOST the call is
+ * synchronous; with TC_MEM_DEVICE it is ordered on opts->stream and returns once enqueued. */
+TC_API int tc_decode(tc_decoder* dec, size_t n_cb, const tc_code_block* cbs, size_t llr_len,
+              const float* llr, size_t post_len, float* posterior, uint8_t* crc_ok,
+              uint32_t* iterations_used, const tc_decode_options* opts);
+
+/* ---------------- kernel accounting (new) ----------------
+ * Every kernel launch is counted.  With timing on, each SISO half-iteration launch is
+ * bracketed by CUDA events on its launching stream; tc_decoder_timing waits for those events
+ * and returns the sums (optionally resetting them). */
+typedef struct {
+  uint64_t launches;      /* kernels launched by this decoder                  */
+  uint64_t siso_launches; /* SISO launches timed                               */
+  double siso_ms;         /* summed device time of the timed SISO launches     */
+  uint64_t trellis_steps; /* output trellis steps (sum of K) of those launches */
+} tc_timing;
+TC_API int tc_decoder_set_timing(tc_decoder* dec, int enable);
+TC_API int tc_decoder_timing(tc_decoder* dec, tc_timing* out, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,396 @@
+// decoder.cu -- the plain (host-driven) GPU turbo decoder and its device buffers.
+//
+// One tc_decode call decodes any number of code blocks of any LTE sizes.  Per full iteration
+// the host enqueues two launches (upper SISO over natural order, lower SISO over QPP order) and,
+// with early stop, one CRC24B launch; every thread owns one window of one code block.  This is
+// the replacement of the reference's Stage 1/2 host loops (lte_turbo_cuda.cu:1391-1540,
+// 1719-1899), batched over code blocks and correct for every K.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "decoder.hpp"
+#include "lte_codec.hpp"
+#include "siso.cuh"
+
+namespace tcb {
+
+namespace {
+
+constexpr int kThreads = 128;  // threads (windows) per block of the plain SISO kernel
+
+template <int S, bool LOWER, bool GLOBAL_CKPT>
+__global__ void __launch_bounds__(kThreads) siso_plain_kernel(const DevCb* __restrict__ cbs,
+                                                              const int32_t* __restrict__ win_cb,
+                                                              int n_win, SisoIo io,
+                                                              const uint8_t* __restrict__ done,
+                                                              float4* ckpt_global,
+                                                              int ckpt_per_thread) {
+  extern __shared__ float4 smem_ckpt[];
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_win) return;
+  const int c = win_cb[g];
+  if (done != nullptr && done[c]) return;
+  const DevCb cb = cbs[c];
+  const int w = g - cb.win0;
+  if (GLOBAL_CKPT) {
+    CkptGlobal ck{ckpt_global + static_cast<int64_t>(2) * ckpt_per_thread * g};
+    siso_window<S, LOWER>(cb, w, g, io, ck);
+  } else {
+    CkptSmem ck{smem_ckpt, static_cast<int>(blockDim.x), static_cast<int>(threadIdx.x)};
+    siso_window<S, LOWER>(cb, w, g, io, ck);
+  }
+}
+
+// sys_i[i] = d0[Pi(i)]; E2 = 0 (first a-priori); one thread per (block, position).
+__global__ void setup_kernel(const DevCb* __restrict__ cbs, const int64_t* __restrict__ cb_start,
+                             int n_cb, int64_t total, const float* __restrict__ llr,
+                             const uint16_t* __restrict__ perm, float* __restrict__ sys_i,
+                             float* __restrict__ e2) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  // binary search of the owning block
+  int lo = 0, hi = n_cb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (cb_start[mid] <= i) lo = mid; else hi = mid - 1;
+  }
+  const DevCb cb = cbs[lo];
+  const int64_t p = i - cb_start[lo];
+  sys_i[cb.work + p] = llr[cb.llr + perm[cb.tab + p]];
+  e2[cb.work + p] = 0.0f;
+}
+
+// CRC24B early stop (lte_turbo.cpp:792-804): hard decisions (>= 0 -> 1) of bits
+// [filler, K) must form a codeword of the reference's CRC24B generator, i.e. the XOR of
+// x^(N-1-i) mod g over the set bits i must be zero.  One warp per code block.
+__global__ void crc_stop_kernel(const DevCb* __restrict__ cbs, int n_cb,
+                                const float* __restrict__ post, const uint32_t* __restrict__ xpow,
+                                uint8_t* __restrict__ done, uint32_t* __restrict__ iters, int it) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n_cb || done[warp]) return;
+  const DevCb cb = cbs[warp];
+  const int n = cb.k - cb.filler;
+  const float* p = post + cb.out + cb.filler;
+  uint32_t syn = 0;
+  for (int i = lane; i < n; i += 32)
+    if (p[i] >= 0.0f) syn ^= xpow[n - 1 - i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) syn ^= __shfl_xor_sync(0xffffffffu, syn, o);
+  if (lane == 0) {
+    iters[warp] = static_cast<uint32_t>(it + 1);
+    if (syn == 0) done[warp] = 1;
+  }
+}
+
+__global__ void init_flags_kernel(int n_cb, uint8_t* __restrict__ done, uint32_t* __restrict__ iters,
+                                  uint32_t max_iterations) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_cb) {
+    done[i] = 0;
+    iters[i] = max_iterations;  // early stop lowers it
+  }
+}
+
+__global__ void finish_kernel(int n_cb, const uint8_t* __restrict__ done, uint8_t* crc_ok,
+                              int early_stop) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_cb) crc_ok[i] = early_stop ? done[i] : 0;
+}
+
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess)
+    throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class T>
+T* grow(DeviceBuffer& b, size_t count) {
+  b.reserve(count * sizeof(T));
+  return static_cast<T*>(b.ptr);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+void DeviceBuffer::reserve(size_t need) {
+  if (need <= bytes) return;
+  release();
+  size_t n = std::max<size_t>(need, 256);
+  n = n + n / 4;  // headroom for slightly larger later calls
+  cudaError_t e = cudaMalloc(&ptr, n);
+  if (e != cudaSuccess) {
+    ptr = nullptr;
+    bytes = 0;
+    throw CudaError(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  bytes = n;
+}
+
+void DeviceBuffer::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+Decoder::Decoder(int device) : device_(device) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+    throw NoDevice("no CUDA device is visible");
+  if (device < 0 || device >= count) throw InvalidArgument("device index out of range");
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  cudaStream_t own = nullptr;
+  check(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking), "cudaStreamCreate");
+  stream_ = own;
+  cudaDeviceProp prop{};
+  check(cudaGetDeviceProperties(&prop, device_), "cudaGetDeviceProperties");
+  sm_count_ = prop.multiProcessorCount;
+  smem_optin_ = static_cast<int>(prop.sharedMemPerBlockOptin);
+
+  // QPP permutation tables for all 188 block sizes, uint16 per position.
+  std::vector<uint16_t> perm, inv;
+  tab_offset_.resize(kQppCount);
+  for (int i = 0; i < kQppCount; ++i) {
+    const QppEntry e = qpp_entry(i);
+    tab_offset_[i] = static_cast<int32_t>(perm.size());
+    const auto p = qpp_permutation(e.k);
+    std::vector<uint16_t> iv(e.k);
+    for (int32_t j = 0; j < e.k; ++j) {
+      perm.push_back(static_cast<uint16_t>(p[j]));
+      iv[p[j]] = static_cast<uint16_t>(j);
+    }
+    inv.insert(inv.end(), iv.begin(), iv.end());
+  }
+  // x^j mod g_CRC24B for j < 6144
+  std::vector<uint32_t> xpow(6144);
+  const uint32_t g = crc_generator_mask(CrcKind::Crc24B);
+  uint32_t r = 1;
+  for (int j = 0; j < 6144; ++j) {
+    xpow[j] = r;
+    r <<= 1;
+    if (r & (1u << 24)) r ^= (1u << 24) | g;
+  }
+  d_perm_.reserve(perm.size() * 2);
+  d_inv_.reserve(inv.size() * 2);
+  d_xpow_.reserve(xpow.size() * 4);
+  check(cudaMemcpy(d_perm_.ptr, perm.data(), perm.size() * 2, cudaMemcpyHostToDevice), "upload perm");
+  check(cudaMemcpy(d_inv_.ptr, inv.data(), inv.size() * 2, cudaMemcpyHostToDevice), "upload inv");
+  check(cudaMemcpy(d_xpow_.ptr, xpow.data(), xpow.size() * 4, cudaMemcpyHostToDevice), "upload crc");
+
+  const int smem = smem_optin_;
+  check(cudaFuncSetAttribute(siso_plain_kernel<kSub, false, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
+  check(cudaFuncSetAttribute(siso_plain_kernel<kSub, true, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
+}
+
+Decoder::~Decoder() {
+  cudaSetDevice(device_);
+  for (auto& e : events_) {
+    if (e.start) cudaEventDestroy(static_cast<cudaEvent_t>(e.start));
+    if (e.stop) cudaEventDestroy(static_cast<cudaEvent_t>(e.stop));
+  }
+  if (stream_) cudaStreamDestroy(static_cast<cudaStream_t>(stream_));
+  for (DeviceBuffer* b : {&d_perm_, &d_inv_, &d_xpow_, &d_cbs_, &d_wincb_, &d_start_, &d_llr_,
+                          &d_sysi_, &d_e1i_, &d_e2_, &d_post_, &d_seed_, &d_done_, &d_iters_,
+                          &d_crc_, &d_ckpt_})
+    b->release();
+}
+
+void Decoder::set_timing(bool on) {
+  std::lock_guard<std::mutex> lock(mu_);
+  timing_on_ = on;
+}
+
+void Decoder::record_start(void* stream) {
+  if (!timing_on_) return;
+  if (events_used_ == events_.size()) {
+    EventPair p;
+    cudaEvent_t a, b;
+    check(cudaEventCreate(&a), "cudaEventCreate");
+    check(cudaEventCreate(&b), "cudaEventCreate");
+    p.start = a;
+    p.stop = b;
+    events_.push_back(p);
+  }
+  check(cudaEventRecord(static_cast<cudaEvent_t>(events_[events_used_].start),
+                        static_cast<cudaStream_t>(stream)), "cudaEventRecord");
+}
+
+void Decoder::record_stop(void* stream, uint64_t steps) {
+  if (!timing_on_) return;
+  EventPair& p = events_[events_used_++];
+  p.steps = steps;
+  check(cudaEventRecord(static_cast<cudaEvent_t>(p.stop), static_cast<cudaStream_t>(stream)),
+        "cudaEventRecord");
+}
+
+Timing Decoder::timing(bool reset) {
+  std::lock_guard<std::mutex> lock(mu_);
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  for (size_t i = 0; i < events_used_; ++i) {
+    float ms = 0.0f;
+    check(cudaEventSynchronize(static_cast<cudaEvent_t>(events_[i].stop)), "cudaEventSynchronize");
+    check(cudaEventElapsedTime(&ms, static_cast<cudaEvent_t>(events_[i].start),
+                               static_cast<cudaEvent_t>(events_[i].stop)), "cudaEventElapsedTime");
+    timing_.siso_ms += ms;
+    timing_.siso_launches += 1;
+    timing_.trellis_steps += events_[i].steps;
+  }
+  events_used_ = 0;
+  const Timing t = timing_;
+  if (reset) timing_ = Timing{};
+  return t;
+}
+
+int Decoder::pick_window(int32_t k, int32_t requested) const {
+  if (requested > 0) return std::min<int32_t>(requested, k);
+  return std::min<int32_t>(kDefaultWindow, k);
+}
+
+void Decoder::decode(const DecodeRequest& rq) {
+  std::lock_guard<std::mutex> lock(mu_);
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  cudaStream_t st = static_cast<cudaStream_t>(rq.stream ? rq.stream : stream_);
+  const size_t n = rq.n_cb;
+  if (n == 0) return;
+
+  // ---- validate and lay out ----
+  if (reinterpret_cast<uintptr_t>(rq.llr) % 16 != 0)
+    throw InvalidArgument("the LLR buffer must be 16-byte aligned");
+  const int guard = rq.guard < 0 ? kDefaultGuard : rq.guard;
+  if (guard % kSub != 0) throw InvalidArgument("guard must be a multiple of 8");
+  std::vector<DevCb> cbs(n);
+  std::vector<int64_t> start(n);
+  std::vector<int32_t> wincb;
+  int64_t work = 0;
+  int max_ckpt = 0;
+  for (size_t i = 0; i < n; ++i) {
+    const int32_t k = rq.cbs[i].k;
+    const int qi = qpp_index(k);
+    if (qi < 0) throw OutOfRange("unsupported QPP block size");
+    if (rq.cbs[i].filler < 0 || rq.cbs[i].filler >= k) throw InvalidArgument("invalid filler count");
+    if (rq.cbs[i].llr_offset < 0 || rq.cbs[i].llr_offset % 4 != 0 ||
+        static_cast<size_t>(rq.cbs[i].llr_offset) + 3 * static_cast<size_t>(k + 4) > rq.llr_len)
+      throw InvalidArgument("invalid LLR offset (must be a multiple of 4 and in range)");
+    if (rq.cbs[i].out_offset < 0 ||
+        static_cast<size_t>(rq.cbs[i].out_offset) + static_cast<size_t>(k) > rq.post_len)
+      throw InvalidArgument("invalid posterior offset");
+    DevCb& d = cbs[i];
+    d.k = k;
+    d.filler = rq.cbs[i].filler;
+    d.tab = tab_offset_[qi];
+    d.window = pick_window(k, rq.window);
+    if (d.window % kSub != 0) throw InvalidArgument("window must be a multiple of 8");
+    if (guard > d.window && d.window < k) throw InvalidArgument("guard must not exceed the window");
+    d.nwin = (k + d.window - 1) / d.window;
+    d.win0 = static_cast<int32_t>(wincb.size());
+    d.llr = rq.cbs[i].llr_offset;
+    d.work = work;
+    d.out = rq.cbs[i].out_offset;
+    start[i] = work;
+    work += k;
+    max_ckpt = std::max(max_ckpt, d.window / kSub);
+    for (int w = 0; w < d.nwin; ++w) wincb.push_back(static_cast<int32_t>(i));
+  }
+  const int n_win = static_cast<int>(wincb.size());
+  const size_t ckpt_bytes = static_cast<size_t>(kThreads) * max_ckpt * 32;
+  const bool global_ckpt = ckpt_bytes > static_cast<size_t>(smem_optin_);
+
+  // ---- device buffers ----
+  DevCb* dcbs = grow<DevCb>(d_cbs_, n);
+  int32_t* dwin = grow<int32_t>(d_wincb_, n_win);
+  int64_t* dstart = grow<int64_t>(d_start_, n);
+  float* sysi = grow<float>(d_sysi_, work);
+  float* e1i = grow<float>(d_e1i_, work);
+  float* e2 = grow<float>(d_e2_, work);
+  float* seeds = grow<float>(d_seed_, static_cast<size_t>(n_win) * 16 * 4);
+  uint8_t* done = grow<uint8_t>(d_done_, n);
+  uint32_t* iters = (rq.device_memory && rq.iterations_used) ? rq.iterations_used
+                                                              : grow<uint32_t>(d_iters_, n);
+  uint8_t* crc = (rq.device_memory && rq.crc_ok) ? rq.crc_ok : grow<uint8_t>(d_crc_, n);
+  const float* llr = rq.llr;
+  float* post = rq.posterior;
+  if (!rq.device_memory) {
+    float* dl = grow<float>(d_llr_, rq.llr_len);
+    check(cudaMemcpyAsync(dl, rq.llr, rq.llr_len * sizeof(float), cudaMemcpyHostToDevice, st),
+          "copy LLRs in");
+    llr = dl;
+    post = grow<float>(d_post_, rq.post_len);
+    // positions outside every block's range come back as 0
+    check(cudaMemsetAsync(post, 0, rq.post_len * sizeof(float), st), "zero posterior");
+  }
+  float4* ckpt = nullptr;
+  if (global_ckpt) ckpt = grow<float4>(d_ckpt_, static_cast<size_t>(n_win) * 2 * max_ckpt);
+
+  check(cudaMemcpyAsync(dcbs, cbs.data(), n * sizeof(DevCb), cudaMemcpyHostToDevice, st), "copy cbs");
+  check(cudaMemcpyAsync(dwin, wincb.data(), n_win * sizeof(int32_t), cudaMemcpyHostToDevice, st),
+        "copy windows");
+  check(cudaMemcpyAsync(dstart, start.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, st),
+        "copy starts");
+  check(cudaMemsetAsync(seeds, 0, static_cast<size_t>(n_win) * 16 * 4 * sizeof(float), st), "zero seeds");
+  init_flags_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(
+      static_cast<int>(n), done, iters, rq.max_iterations);
+  check(cudaGetLastError(), "init launch");
+
+  const uint16_t* dperm = static_cast<const uint16_t*>(d_perm_.ptr);
+  const uint16_t* dinv = static_cast<const uint16_t*>(d_inv_.ptr);
+  timing_.launches += 3;  // init, setup, finish
+  setup_kernel<<<static_cast<unsigned>((work + 255) / 256), 256, 0, st>>>(
+      dcbs, dstart, static_cast<int>(n), work, llr, dperm, sysi, e2);
+  check(cudaGetLastError(), "setup launch");
+
+  const int blocks = (n_win + kThreads - 1) / kThreads;
+  const size_t smem = global_ckpt ? 0 : ckpt_bytes;
+  const size_t seed_slab = static_cast<size_t>(n_win) * 16;
+  float* seed_up[2] = {seeds, seeds + seed_slab};
+  float* seed_lo[2] = {seeds + 2 * seed_slab, seeds + 3 * seed_slab};
+  for (uint32_t it = 0; it < rq.max_iterations; ++it) {
+    const float s_up = rq.scales ? rq.scales[2 * it] : 1.0f;
+    const float s_lo = rq.scales ? rq.scales[2 * it + 1] : 1.0f;
+    SisoIo up{llr, sysi, e2, e1i, nullptr, dperm, dinv, seed_up[it & 1], seed_up[(it + 1) & 1],
+              s_up, guard};
+    SisoIo lo{llr, sysi, e1i, e2, post, dperm, dinv, seed_lo[it & 1], seed_lo[(it + 1) & 1],
+              s_lo, guard};
+    const uint8_t* dn = rq.early_stop ? done : nullptr;
+    for (int half = 0; half < 2; ++half) {
+      const SisoIo& io = half ? lo : up;
+      record_start(st);
+      if (global_ckpt) {
+        if (half) siso_plain_kernel<kSub, true, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, dn, ckpt, max_ckpt);
+        else siso_plain_kernel<kSub, false, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, dn, ckpt, max_ckpt);
+      } else {
+        if (half) siso_plain_kernel<kSub, true, false><<<blocks, kThreads, smem, st>>>(dcbs, dwin, n_win, io, dn, nullptr, 0);
+        else siso_plain_kernel<kSub, false, false><<<blocks, kThreads, smem, st>>>(dcbs, dwin, n_win, io, dn, nullptr, 0);
+      }
+      check(cudaGetLastError(), "SISO launch");
+      record_stop(st, static_cast<uint64_t>(work));
+      timing_.launches += 1;
+    }
+    if (rq.early_stop) {
+      crc_stop_kernel<<<static_cast<unsigned>((n * 32 + 255) / 256), 256, 0, st>>>(
+          dcbs, static_cast<int>(n), post, static_cast<const uint32_t*>(d_xpow_.ptr), done, iters,
+          static_cast<int>(it));
+      check(cudaGetLastError(), "CRC launch");
+      timing_.launches += 1;
+    }
+  }
+  finish_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(static_cast<int>(n), done, crc,
+                                                                         rq.early_stop ? 1 : 0);
+  check(cudaGetLastError(), "finish launch");
+  if (!rq.device_memory) {
+    check(cudaMemcpyAsync(rq.posterior, post, rq.post_len * sizeof(float), cudaMemcpyDeviceToHost, st),
+          "copy posterior out");
+    if (rq.crc_ok) check(cudaMemcpyAsync(rq.crc_ok, crc, n, cudaMemcpyDeviceToHost, st), "copy crc out");
+    if (rq.iterations_used)
+      check(cudaMemcpyAsync(rq.iterations_used, iters, n * 4, cudaMemcpyDeviceToHost, st), "copy iters out");
+    check(cudaStreamSynchronize(st), "sync");
+  }
+}
+
+}  // namespace tcb

@@ -1,0 +1,117 @@
+// decoder.hpp -- host-side objects of the GPU decoder (no CUDA types in the interface).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace tcb {
+
+// Error classes; the C ABI maps each to a status code, the C++ API rethrows the reference's
+// exception types (std::invalid_argument, std::out_of_range, std::runtime_error).
+struct InvalidArgument : std::invalid_argument {
+  using std::invalid_argument::invalid_argument;
+};
+struct OutOfRange : std::out_of_range {
+  using std::out_of_range::out_of_range;
+};
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct NoDevice : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct DeviceTimeout : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct CapacityExceeded : std::length_error {
+  using std::length_error::length_error;
+};
+
+constexpr int kSub = 8;              // alpha checkpoint interval (steps)
+constexpr int kDefaultWindow = 128;  // window length (steps)
+constexpr int kDefaultGuard = 64;    // warm-up steps on each side of a window
+
+struct CodeBlockDesc {
+  int32_t k;
+  int32_t filler;
+  int64_t llr_offset;  // floats; [d0|d1|d2], 3*(K+4) floats, multiple of 4
+  int64_t out_offset;  // floats; K posterior LLRs
+};
+
+struct DecodeRequest {
+  size_t n_cb = 0;
+  const CodeBlockDesc* cbs = nullptr;  // host memory
+  size_t llr_len = 0;
+  const float* llr = nullptr;
+  size_t post_len = 0;
+  float* posterior = nullptr;
+  uint8_t* crc_ok = nullptr;
+  uint32_t* iterations_used = nullptr;
+  uint32_t max_iterations = 8;
+  bool early_stop = false;
+  int window = 0;   // 0: default
+  int guard = -1;   // <0: default
+  bool device_memory = false;  // llr/posterior/crc_ok/iterations_used are device pointers
+  const float* scales = nullptr;  // host; 2 per iteration (upper, lower); null = all 1
+  void* stream = nullptr;
+};
+
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  void reserve(size_t need);  // grows (discarding contents) when too small
+  void release();
+};
+
+// Kernel accounting: every launch is counted; with timing on, each SISO launch is bracketed by
+// CUDA events on the launching stream and the elapsed times are summed on request.
+struct Timing {
+  uint64_t launches = 0;       // kernels launched by this decoder
+  uint64_t siso_launches = 0;  // SISO half-iteration launches timed
+  double siso_ms = 0.0;        // summed device time of the timed SISO launches
+  uint64_t trellis_steps = 0;  // output trellis steps of the timed SISO launches
+};
+
+class Decoder {
+ public:
+  explicit Decoder(int device);
+  ~Decoder();
+  Decoder(const Decoder&) = delete;
+  Decoder& operator=(const Decoder&) = delete;
+
+  void decode(const DecodeRequest& rq);  // plain schedule
+  int device() const { return device_; }
+  void set_timing(bool on);
+  Timing timing(bool reset);  // waits for the recorded events
+  int sm_count() const { return sm_count_; }
+
+ private:
+  int pick_window(int32_t k, int32_t requested) const;
+  void record_start(void* stream);
+  void record_stop(void* stream, uint64_t steps);
+
+  struct EventPair {
+    void* start = nullptr;
+    void* stop = nullptr;
+    uint64_t steps = 0;
+  };
+  bool timing_on_ = false;
+  Timing timing_;
+  std::vector<EventPair> events_;   // pool
+  size_t events_used_ = 0;
+
+  std::mutex mu_;
+  int device_ = 0;
+  int sm_count_ = 0;
+  int smem_optin_ = 0;
+  void* stream_ = nullptr;  // cudaStream_t
+  std::vector<int32_t> tab_offset_;
+  DeviceBuffer d_perm_, d_inv_, d_xpow_;
+  DeviceBuffer d_cbs_, d_wincb_, d_start_, d_llr_, d_sysi_, d_e1i_, d_e2_, d_post_, d_seed_,
+      d_done_, d_iters_, d_crc_, d_ckpt_;
+};
+
+}  // namespace tcb

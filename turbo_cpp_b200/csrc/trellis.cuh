@@ -1,0 +1,136 @@
+// trellis.cuh -- device-side exact Log-MAP arithmetic for the LTE constituent code.
+//
+// Metrics are kept in the base-2 log domain (natural-log metric * log2(e)), so that the
+// Jacobian logarithm max*(x, y) = max(x, y) + log2(1 + 2^-|x-y|) costs one ex2 and one lg2
+// (the MUFU instructions ex2.approx / lg2.approx) and no scaling multiplies.  The branch metric
+// of the reference, 0.5 * (+-(Ls+La) +- Lp) (lte_turbo.cpp:437-438), becomes +-a +-b with
+// a = 0.5*log2(e)*(Ls+La) and b = 0.5*log2(e)*Lp.
+//
+// Trellis (lte_turbo.cpp:333-341): state = (s2 s1 s0), feedback fb = u^s1^s2, parity
+// fb^s0^s2, next state (fb s2 s1).  Hence next state n = (n2 n1 n0) is reached with input
+// u = n2^n1^n0 from the two predecessors 2*(n&3) + s0, s0 in {0,1}, whose parities are
+// n2^n1^s0.  All state/branch indexing below is resolved at compile time.
+#pragma once
+#include <cstdint>
+
+namespace tcb {
+
+constexpr float kLog2e = 1.4426950408889634f;
+constexpr float kLn2 = 0.6931471805599453f;
+constexpr float kHalfLog2e = 0.5f * kLog2e;
+// Stand-in for -infinity: finite, so that max*(-inf, -inf) stays well defined
+// (d = 0 instead of NaN) while 2^(kNegBig - m) underflows to exactly 0.
+constexpr float kNegBig = -1.0e30f;
+
+__device__ __forceinline__ float ex2(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float lg2(float x) {
+  float y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Jacobian logarithm in base 2: log2(2^x + 2^y).
+__device__ __forceinline__ float max_star(float x, float y) {
+  const float m = fmaxf(x, y);
+  const float d = fabsf(x - y);
+  return m + lg2(1.0f + ex2(-d));
+}
+
+__host__ __device__ constexpr int next_state(int s, int u) {
+  return ((u ^ ((s >> 1) & 1) ^ ((s >> 2) & 1)) << 2) | (((s >> 2) & 1) << 1) | ((s >> 1) & 1);
+}
+__host__ __device__ constexpr int parity(int s, int u) {
+  return (u ^ ((s >> 1) & 1) ^ ((s >> 2) & 1)) ^ (s & 1) ^ ((s >> 2) & 1);
+}
+// branch metric +-a +-b for input u and parity p: g0 = a+b, g1 = a-b
+__device__ __forceinline__ float branch(int u, int p, float g0, float g1) {
+  return u ? (p ? g0 : g1) : (p ? -g1 : -g0);
+}
+
+// alpha_{t+1} from alpha_t (in place); normalised so that state 0 is 0.
+__device__ __forceinline__ void alpha_step(float (&al)[8], float a, float b) {
+  const float g0 = a + b, g1 = a - b;
+  float an[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) {
+    const int n2 = (n >> 2) & 1, n1 = (n >> 1) & 1, n0 = n & 1;
+    const int u = n2 ^ n1 ^ n0;
+    const int p0 = 2 * (n & 3);
+    an[n] = max_star(al[p0] + branch(u, n2 ^ n1, g0, g1),
+                     al[p0 + 1] + branch(u, n2 ^ n1 ^ 1, g0, g1));
+  }
+  const float r = an[0];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) al[s] = an[s] - r;
+}
+
+// beta_t from beta_{t+1} (in place); normalised so that state 0 is 0.
+__device__ __forceinline__ void beta_step(float (&be)[8], float a, float b) {
+  const float g0 = a + b, g1 = a - b;
+  float bn[8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s)
+    bn[s] = max_star(be[next_state(s, 0)] + branch(0, parity(s, 0), g0, g1),
+                     be[next_state(s, 1)] + branch(1, parity(s, 1), g0, g1));
+  const float r = bn[0];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) be[s] = bn[s] - r;
+}
+
+// Extrinsic LLR (base-2) of one step: log-sum over the u=1 branches minus log-sum over the
+// u=0 branches of alpha_t + beta_{t+1} +- b.  The +-a part is common to each side and is the
+// (Ls+La) term the reference subtracts again (lte_turbo.cpp:483), so it is left out.
+// Each 8-way log-sum is max + lg2(sum 2^(m - max)): 8 ex2 + 1 lg2 instead of 7 pairwise max*.
+__device__ __forceinline__ float extrinsic2(const float (&al)[8], const float (&be)[8], float b) {
+  float m0[8], m1[8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    m0[s] = al[s] + be[next_state(s, 0)] + (parity(s, 0) ? b : -b);
+    m1[s] = al[s] + be[next_state(s, 1)] + (parity(s, 1) ? b : -b);
+  }
+  float x0 = fmaxf(fmaxf(fmaxf(m0[0], m0[1]), fmaxf(m0[2], m0[3])),
+                   fmaxf(fmaxf(m0[4], m0[5]), fmaxf(m0[6], m0[7])));
+  float x1 = fmaxf(fmaxf(fmaxf(m1[0], m1[1]), fmaxf(m1[2], m1[3])),
+                   fmaxf(fmaxf(m1[4], m1[5]), fmaxf(m1[6], m1[7])));
+  float s0 = 0.0f, s1 = 0.0f;
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    s0 += ex2(m0[s] - x0);
+    s1 += ex2(m1[s] - x1);
+  }
+  return (x1 - x0) + (lg2(s1) - lg2(s0));
+}
+
+// beta at the block end from the three termination steps (lte_turbo.cpp:343-378): from each
+// state the tail input is s1^s2 (feedback 0), which drives every state to 0 in three steps.
+// ts/tp are the tail systematic / parity LLRs in the reference's mapping.
+__device__ __forceinline__ void tail_beta(float (&be)[8], const float ts[3], const float tp[3]) {
+#pragma unroll
+  for (int s0 = 0; s0 < 8; ++s0) {
+    int s = s0;
+    float m = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const int u = ((s >> 1) & 1) ^ ((s >> 2) & 1);
+      const int p = parity(s, u);
+      m += (u ? ts[i] : -ts[i]) + (p ? tp[i] : -tp[i]);
+      s = next_state(s, u);
+    }
+    be[s0] = m * kHalfLog2e;
+  }
+  const float r = be[0];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) be[s] -= r;
+}
+
+__device__ __forceinline__ void alpha_start(float (&al)[8]) {
+  al[0] = 0.0f;
+#pragma unroll
+  for (int s = 1; s < 8; ++s) al[s] = kNegBig;
+}
+
+}  // namespace tcb
