@@ -48,7 +48,7 @@ MUFU_PER_SM_CLK = 16  # B200 SFU lanes per SM per clock (4 per SM sub-partition)
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=14)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--n-cb", type=int, default=4096)
@@ -102,7 +102,7 @@ def max_over_ranks(x: float, world: int) -> float:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms while running."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -116,7 +116,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -240,7 +240,7 @@ def workload_config(args):
                     f"{args.n_cb} code blocks per call, exact Log-MAP, {args.iterations} "
                     "iterations, no early stop, Eb/N0 0.0..1.2 dB step 0.2",
         "n_cb": args.n_cb, "k": K, "iterations": args.iterations,
-        "window": args.window or 128, "guard": 64 if args.guard < 0 else args.guard,
+        "window": args.window or 128, "guard": 96 if args.guard < 0 else args.guard,
         "schedule": args.schedule, "ebn0_db": EBN0[:args.points],
         "l2": "inputs 302 MB per step > 126 MB L2 (no flush needed)",
     }
@@ -276,7 +276,9 @@ def main():
         batches.append(torch.from_numpy(llr).to(f"cuda:{local}"))
         truth.append(bits)
     post = torch.empty(post_len, dtype=torch.float32, device=f"cuda:{local}")
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream(device=local)
+    stream.wait_stream(torch.cuda.current_stream())
+    torch.cuda.set_stream(stream)
 
     def step(i):
         x = batches[i % len(batches)]

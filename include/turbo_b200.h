@@ -115,11 +115,12 @@ typedef struct {
   uint32_t max_iterations; /* default 8                                                   */
   uint32_t early_stop;     /* stop a block once its hard decisions pass CRC24B            */
   int32_t window;          /* steps per window; 0 = default (128); >= K = full trellis    */
-  int32_t guard;           /* warm-up steps on each side; < 0 = default (64); multiple of 8 */
+  int32_t guard;           /* warm-up steps on each side; < 0 = default (96); multiple of 8 */
   uint32_t memory;         /* TC_MEM_HOST (synchronous, copies inside) or TC_MEM_DEVICE   */
   uint32_t schedule;       /* TC_SCHEDULE_PLAIN or TC_SCHEDULE_PERSISTENT                 */
   const float* scales;     /* host array, 2 per iteration (upper, lower); NULL = 1.0     */
-  void* stream;            /* cudaStream_t for TC_MEM_DEVICE; NULL = the decoder's stream */
+  void* stream;            /* cudaStream_t; TC_MEM_DEVICE: used as given (NULL = the legacy
+                              default stream); TC_MEM_HOST: NULL = the decoder's own stream */
 } tc_decode_options;
 
 TC_API int tc_decode_options_init(tc_decode_options* opts);

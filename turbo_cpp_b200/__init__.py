@@ -439,7 +439,7 @@ class DecodeOptions:
     max_iterations: int = 8
     early_stop: bool = False
     window: int = 0          # 0: default (128); >= K: full trellis
-    guard: int = -1          # <0: default (64)
+    guard: int = -1          # <0: default (96)
     schedule: int = SCHEDULE_PLAIN
     scales: Optional[Sequence[float]] = None  # 2 per iteration; None = 1.0
 
@@ -527,7 +527,8 @@ class Decoder:
     def decode_device(self, cbs, n_cb: int, llr_ptr: int, llr_len: int, post_ptr: int,
                       post_len: int, crc_ptr: int = 0, iters_ptr: int = 0,
                       options: Optional[DecodeOptions] = None, stream: int = 0) -> None:
-        """Device pointers (e.g. torch tensors' data_ptr()); ordered on ``stream``."""
+        """Device pointers (e.g. torch tensors' data_ptr()); ordered on ``stream`` (a
+        cudaStream_t as an int; 0 = the legacy default stream)."""
         o = options or DecodeOptions()
         opt, _keep = self._opts(o, MEM_DEVICE, stream)
         _call("tc_decode", self._h, int(n_cb), C.addressof(cbs), int(llr_len), llr_ptr,

@@ -256,7 +256,10 @@ int Decoder::pick_window(int32_t k, int32_t requested) const {
 void Decoder::decode(const DecodeRequest& rq) {
   std::lock_guard<std::mutex> lock(mu_);
   check(cudaSetDevice(device_), "cudaSetDevice");
-  cudaStream_t st = static_cast<cudaStream_t>(rq.stream ? rq.stream : stream_);
+  // device memory: the caller's stream as given (NULL = legacy default stream, as in CUDA);
+  // host memory: the caller's stream if given, else the decoder's own stream
+  cudaStream_t st = static_cast<cudaStream_t>(rq.device_memory ? rq.stream
+                                                               : (rq.stream ? rq.stream : stream_));
   const size_t n = rq.n_cb;
   if (n == 0) return;
 

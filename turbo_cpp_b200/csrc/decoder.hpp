@@ -32,7 +32,7 @@ struct CapacityExceeded : std::length_error {
 
 constexpr int kSub = 8;              // alpha checkpoint interval (steps)
 constexpr int kDefaultWindow = 128;  // window length (steps)
-constexpr int kDefaultGuard = 64;    // warm-up steps on each side of a window
+constexpr int kDefaultGuard = 96;    // warm-up steps on each side of a window
 
 struct CodeBlockDesc {
   int32_t k;
