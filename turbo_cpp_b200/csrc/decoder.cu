@@ -22,10 +22,12 @@ namespace tcb {
 
 namespace {
 
-constexpr int kThreads = 128;  // threads (windows) per block of the plain SISO kernel
+constexpr int kThreads = 64;  // threads (windows) per block of the plain SISO kernel
+constexpr int kMinBlocks = 10;  // 20 warps per SM: at most 96 registers per thread
 
-template <int S, bool LOWER, bool GLOBAL_CKPT>
-__global__ void __launch_bounds__(kThreads) siso_plain_kernel(const DevCb* __restrict__ cbs,
+// KIND: 0 = upper SISO, 1 = lower SISO, 2 = lower SISO that also writes the posterior
+template <int S, int KIND, bool GLOBAL_CKPT>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) siso_plain_kernel(const DevCb* __restrict__ cbs,
                                                               const int32_t* __restrict__ win_cb,
                                                               int n_win, SisoIo io,
                                                               const uint8_t* __restrict__ done,
@@ -40,10 +42,10 @@ __global__ void __launch_bounds__(kThreads) siso_plain_kernel(const DevCb* __res
   const int w = g - cb.win0;
   if (GLOBAL_CKPT) {
     CkptGlobal ck{ckpt_global + static_cast<int64_t>(2) * ckpt_per_thread * g};
-    siso_window<S, LOWER>(cb, w, g, io, ck);
+    siso_window<S, KIND != 0, KIND == 2>(cb, w, g, io, ck);
   } else {
     CkptSmem ck{smem_ckpt, static_cast<int>(blockDim.x), static_cast<int>(threadIdx.x)};
-    siso_window<S, LOWER>(cb, w, g, io, ck);
+    siso_window<S, KIND != 0, KIND == 2>(cb, w, g, io, ck);
   }
 }
 
@@ -183,10 +185,17 @@ Decoder::Decoder(int device) : device_(device) {
   check(cudaMemcpy(d_xpow_.ptr, xpow.data(), xpow.size() * 4, cudaMemcpyHostToDevice), "upload crc");
 
   const int smem = smem_optin_;
-  check(cudaFuncSetAttribute(siso_plain_kernel<kSub, false, false>,
+  check(cudaFuncSetAttribute(siso_plain_kernel<kSub, 0, false>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
-  check(cudaFuncSetAttribute(siso_plain_kernel<kSub, true, false>,
+  check(cudaFuncSetAttribute(siso_plain_kernel<kSub, 1, false>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
+  check(cudaFuncSetAttribute(siso_plain_kernel<kSub, 2, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
+  for (const void* f : {reinterpret_cast<const void*>(siso_plain_kernel<kSub, 0, true>),
+                        reinterpret_cast<const void*>(siso_plain_kernel<kSub, 1, true>),
+                        reinterpret_cast<const void*>(siso_plain_kernel<kSub, 2, true>)})
+    check(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 0),
+          "carveout attr");
 }
 
 Decoder::~Decoder() {
@@ -267,7 +276,7 @@ void Decoder::decode(const DecodeRequest& rq) {
   if (reinterpret_cast<uintptr_t>(rq.llr) % 16 != 0)
     throw InvalidArgument("the LLR buffer must be 16-byte aligned");
   const int guard = rq.guard < 0 ? kDefaultGuard : rq.guard;
-  if (guard % kSub != 0) throw InvalidArgument("guard must be a multiple of 8");
+  if (guard % kGroup != 0) throw InvalidArgument("guard must be a multiple of 8");
   std::vector<DevCb> cbs(n);
   std::vector<int64_t> start(n);
   std::vector<int32_t> wincb;
@@ -289,7 +298,7 @@ void Decoder::decode(const DecodeRequest& rq) {
     d.filler = rq.cbs[i].filler;
     d.tab = tab_offset_[qi];
     d.window = pick_window(k, rq.window);
-    if (d.window % kSub != 0) throw InvalidArgument("window must be a multiple of 8");
+    if (d.window % kGroup != 0) throw InvalidArgument("window must be a multiple of 8");
     if (guard > d.window && d.window < k) throw InvalidArgument("guard must not exceed the window");
     d.nwin = (k + d.window - 1) / d.window;
     d.win0 = static_cast<int32_t>(wincb.size());
@@ -302,8 +311,11 @@ void Decoder::decode(const DecodeRequest& rq) {
     for (int w = 0; w < d.nwin; ++w) wincb.push_back(static_cast<int32_t>(i));
   }
   const int n_win = static_cast<int>(wincb.size());
-  const size_t ckpt_bytes = static_cast<size_t>(kThreads) * max_ckpt * 32;
-  const bool global_ckpt = ckpt_bytes > static_cast<size_t>(smem_optin_);
+  // Checkpoints live in a global scratch slot per window: 8 B of traffic per output step, and
+  // leaving shared memory unused gives the L1 cache the whole 256 KB for the input streams.
+  const size_t ckpt_bytes = static_cast<size_t>(kThreads) * max_ckpt * 2 * sizeof(float4);
+  const bool global_ckpt = rq.smem_checkpoints ? ckpt_bytes > static_cast<size_t>(smem_optin_)
+                                               : true;
 
   // ---- device buffers ----
   DevCb* dcbs = grow<DevCb>(d_cbs_, n);
@@ -361,15 +373,20 @@ void Decoder::decode(const DecodeRequest& rq) {
     SisoIo lo{llr, sysi, e1i, e2, post, dperm, dinv, seed_lo[it & 1], seed_lo[(it + 1) & 1],
               s_lo, guard};
     const uint8_t* dn = rq.early_stop ? done : nullptr;
+    // the posterior is needed after the last iteration and, with early stop, after each one
+    const bool post_now = rq.early_stop || it + 1 == rq.max_iterations;
     for (int half = 0; half < 2; ++half) {
       const SisoIo& io = half ? lo : up;
+      const int kind = half == 0 ? 0 : (post_now ? 2 : 1);
       record_start(st);
       if (global_ckpt) {
-        if (half) siso_plain_kernel<kSub, true, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, dn, ckpt, max_ckpt);
-        else siso_plain_kernel<kSub, false, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, dn, ckpt, max_ckpt);
+        if (kind == 0) siso_plain_kernel<kSub, 0, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, dn, ckpt, max_ckpt);
+        else if (kind == 1) siso_plain_kernel<kSub, 1, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, dn, ckpt, max_ckpt);
+        else siso_plain_kernel<kSub, 2, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, dn, ckpt, max_ckpt);
       } else {
-        if (half) siso_plain_kernel<kSub, true, false><<<blocks, kThreads, smem, st>>>(dcbs, dwin, n_win, io, dn, nullptr, 0);
-        else siso_plain_kernel<kSub, false, false><<<blocks, kThreads, smem, st>>>(dcbs, dwin, n_win, io, dn, nullptr, 0);
+        if (kind == 0) siso_plain_kernel<kSub, 0, false><<<blocks, kThreads, smem, st>>>(dcbs, dwin, n_win, io, dn, nullptr, 0);
+        else if (kind == 1) siso_plain_kernel<kSub, 1, false><<<blocks, kThreads, smem, st>>>(dcbs, dwin, n_win, io, dn, nullptr, 0);
+        else siso_plain_kernel<kSub, 2, false><<<blocks, kThreads, smem, st>>>(dcbs, dwin, n_win, io, dn, nullptr, 0);
       }
       check(cudaGetLastError(), "SISO launch");
       record_stop(st, static_cast<uint64_t>(work));

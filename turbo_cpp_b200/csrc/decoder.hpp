@@ -30,7 +30,8 @@ struct CapacityExceeded : std::length_error {
   using std::length_error::length_error;
 };
 
-constexpr int kSub = 8;              // alpha checkpoint interval (steps)
+constexpr int kSub = 4;              // alpha checkpoint interval (steps)
+constexpr int kGroup = 8;            // load granularity: windows and guards are multiples of 8
 constexpr int kDefaultWindow = 128;  // window length (steps)
 constexpr int kDefaultGuard = 96;    // warm-up steps on each side of a window
 
@@ -55,6 +56,7 @@ struct DecodeRequest {
   int window = 0;   // 0: default
   int guard = -1;   // <0: default
   bool device_memory = false;  // llr/posterior/crc_ok/iterations_used are device pointers
+  bool smem_checkpoints = false;  // alpha checkpoints in shared memory instead of global scratch
   const float* scales = nullptr;  // host; 2 per iteration (upper, lower); null = all 1
   void* stream = nullptr;
 };

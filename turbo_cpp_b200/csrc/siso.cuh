@@ -50,18 +50,35 @@ __device__ __forceinline__ float4 ld4(const float* p) {
   return __ldg(reinterpret_cast<const float4*>(p));
 }
 
-// Loads 4 consecutive steps: raw sys+apr (sa), scaled a and b.
-__device__ __forceinline__ void load_steps4(const float* sys, const float* apr, const float* par,
-                                            int q, float* sa, float* a, float* b) {
-  const float4 s = ld4(sys + q), e = ld4(apr + q), p = ld4(par + q);
-  sa[0] = s.x + e.x; sa[1] = s.y + e.y; sa[2] = s.z + e.z; sa[3] = s.w + e.w;
-  a[0] = kHalfLog2e * sa[0]; a[1] = kHalfLog2e * sa[1];
-  a[2] = kHalfLog2e * sa[2]; a[3] = kHalfLog2e * sa[3];
-  b[0] = kHalfLog2e * p.x; b[1] = kHalfLog2e * p.y; b[2] = kHalfLog2e * p.z; b[3] = kHalfLog2e * p.w;
+// Raw inputs of 4 consecutive steps (one float4 per stream).
+struct Raw4 {
+  float4 s, e, p;  // systematic, a-priori, parity
+};
+__device__ __forceinline__ Raw4 load_raw4(const float* sys, const float* apr, const float* par,
+                                          int q) {
+  return Raw4{ld4(sys + q), ld4(apr + q), ld4(par + q)};
+}
+// raw -> sys+apr (sa), a = c (sys+apr), b = c par with c = log2(e)/2
+__device__ __forceinline__ void scale4(const Raw4& r, float* sa, float* a, float* b) {
+  sa[0] = r.s.x + r.e.x; sa[1] = r.s.y + r.e.y; sa[2] = r.s.z + r.e.z; sa[3] = r.s.w + r.e.w;
+#pragma unroll
+  for (int t = 0; t < 4; ++t) a[t] = kHalfLog2e * sa[t];
+  b[0] = kHalfLog2e * r.p.x; b[1] = kHalfLog2e * r.p.y; b[2] = kHalfLog2e * r.p.z;
+  b[3] = kHalfLog2e * r.p.w;
 }
 
-// Checkpoint storage: shared memory (thread-minor float4 layout, conflict-free) or a global
-// scratch slot.
+// Raw inputs of 8 consecutive steps: both halves of each 32-byte sector are requested back to
+// back, so every sector crosses from L2 once.
+struct Raw8 {
+  Raw4 lo, hi;
+};
+__device__ __forceinline__ Raw8 load_raw8(const float* sys, const float* apr, const float* par,
+                                          int q) {
+  return Raw8{load_raw4(sys, apr, par, q), load_raw4(sys, apr, par, q + 4)};
+}
+
+// Checkpoint storage, 8 floats per checkpoint as two float4.  Shared memory: thread-minor
+// float4 planes (conflict-free); global scratch: a per-thread slot.
 struct CkptSmem {
   float4* base;  // dynamic shared memory
   int stride;    // threads per block
@@ -102,10 +119,11 @@ __device__ __forceinline__ void tail_llrs(const float* d0, int k, float ts[3], f
 }
 
 // Runs window w of block cb for one half-iteration.  g = launch-wide window index (seed slot).
-template <int S, bool LOWER, class Ckpt>
+// POST (lower SISO only): also write the posterior Ls + e1 + e2 (last iteration, early stop).
+template <int S, bool LOWER, bool POST, class Ckpt>
 __device__ __forceinline__ void siso_window(const DevCb& cb, int w, int g, const SisoIo& io,
                                             const Ckpt& ck) {
-  static_assert(S % 4 == 0, "sub-window must be a multiple of 4 steps");
+  static_assert(S == 4, "sub-windows are one float4 group of 4 steps");
   const int K = cb.k, W = cb.window, G = io.guard;
   const int lo = w * W, hi = min(lo + W, K);
   const float* d0 = io.llr + cb.llr;
@@ -113,10 +131,9 @@ __device__ __forceinline__ void siso_window(const DevCb& cb, int w, int g, const
   const float* par = d0 + (LOWER ? 2 : 1) * (K + 4);
   const float* apr = io.apr + cb.work;
   const int nsub = (hi - lo) / S;
-
   float sa[4], a[4], b[4];
 
-  // ---- forward: warm-up, then alpha checkpoints every S steps ----
+  // ---- forward: warm-up from a_lo, then a checkpoint every 4 steps over [lo, hi) ----
   float al[8];
   int a_lo = lo - G;
   if (a_lo <= 0) {
@@ -126,18 +143,20 @@ __device__ __forceinline__ void siso_window(const DevCb& cb, int w, int g, const
     const float4 x = ld4(io.seed_in + 16 * g), y = ld4(io.seed_in + 16 * g + 4);
     al[0] = x.x; al[1] = x.y; al[2] = x.z; al[3] = x.w; al[4] = y.x; al[5] = y.y; al[6] = y.z; al[7] = y.w;
   }
-  for (int q = a_lo; q < lo; q += 4) {
-    load_steps4(sys, apr, par, q, sa, a, b);
-#pragma unroll
-    for (int t = 0; t < 4; ++t) alpha_step(al, a[t], b[t]);
-  }
-  for (int j = 0; j < nsub; ++j) {
-    ck.store(j, al);
-#pragma unroll
-    for (int q4 = 0; q4 < S; q4 += 4) {
-      load_steps4(sys, apr, par, lo + j * S + q4, sa, a, b);
+  {  // 8-step groups (both halves of each sector); the next group is requested early
+    Raw8 cur = load_raw8(sys, apr, par, a_lo);
+    for (int q = a_lo; q < hi; q += 8) {
+      Raw8 nxt = cur;
+      if (q + 8 < hi) nxt = load_raw8(sys, apr, par, q + 8);
+      if (q >= lo) ck.store((q - lo) / S, al);
+      scale4(cur.lo, sa, a, b);
 #pragma unroll
       for (int t = 0; t < 4; ++t) alpha_step(al, a[t], b[t]);
+      if (q >= lo) ck.store((q - lo) / S + 1, al);
+      scale4(cur.hi, sa, a, b);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) alpha_step(al, a[t], b[t]);
+      cur = nxt;
     }
   }
   // seed for window w+1: alpha at hi - G
@@ -154,7 +173,7 @@ __device__ __forceinline__ void siso_window(const DevCb& cb, int w, int g, const
     o[1] = make_float4(r[4], r[5], r[6], r[7]);
   }
 
-  // ---- backward: warm-up, then per sub-window recompute alpha + beta + extrinsic ----
+  // ---- backward: warm-up from b_hi down to hi ----
   float be[8];
   int b_hi = hi + G;
   if (b_hi >= K) {
@@ -166,10 +185,19 @@ __device__ __forceinline__ void siso_window(const DevCb& cb, int w, int g, const
     const float4 x = ld4(io.seed_in + 16 * g + 8), y = ld4(io.seed_in + 16 * g + 12);
     be[0] = x.x; be[1] = x.y; be[2] = x.z; be[3] = x.w; be[4] = y.x; be[5] = y.y; be[6] = y.z; be[7] = y.w;
   }
-  for (int q = b_hi - 4; q >= hi; q -= 4) {
-    load_steps4(sys, apr, par, q, sa, a, b);
+  if (b_hi > hi) {
+    Raw8 cur = load_raw8(sys, apr, par, b_hi - 8);
+    for (int q = b_hi - 8; q >= hi; q -= 8) {
+      Raw8 nxt = cur;
+      if (q - 8 >= hi) nxt = load_raw8(sys, apr, par, q - 8);
+      scale4(cur.hi, sa, a, b);
 #pragma unroll
-    for (int t = 3; t >= 0; --t) beta_step(be, a[t], b[t]);
+      for (int t = 3; t >= 0; --t) beta_step(be, a[t], b[t]);
+      scale4(cur.lo, sa, a, b);
+#pragma unroll
+      for (int t = 3; t >= 0; --t) beta_step(be, a[t], b[t]);
+      cur = nxt;
+    }
   }
   const bool rec_beta = (w > 0) && (lo + G <= hi);
   float4* bseed = rec_beta ? reinterpret_cast<float4*>(io.seed_out + 16 * (g - 1) + 8) : nullptr;
@@ -177,37 +205,47 @@ __device__ __forceinline__ void siso_window(const DevCb& cb, int w, int g, const
     bseed[0] = make_float4(be[0], be[1], be[2], be[3]);
     bseed[1] = make_float4(be[4], be[5], be[6], be[7]);
   }
+
+  // ---- per 4-step sub-window (last to first): recompute alpha, then beta + extrinsic.  The
+  // inputs, permutation indices and checkpoint of the next sub-window are requested one
+  // sub-window ahead. ----
   const uint16_t* pt = (LOWER ? io.perm : io.inv) + cb.tab;
+  Raw4 r_n;
+  uint2 i_n;
+  float c_n[8];
+  if (nsub > 0) {
+    const int base = lo + (nsub - 1) * S;
+    r_n = load_raw4(sys, apr, par, base);
+    i_n = __ldg(reinterpret_cast<const uint2*>(pt + base));
+    ck.load(nsub - 1, c_n);
+  }
   for (int j = nsub - 1; j >= 0; --j) {
     const int base = lo + j * S;
-    float SA[S], A_[S], B_[S];
-#pragma unroll
-    for (int q4 = 0; q4 < S; q4 += 4) load_steps4(sys, apr, par, base + q4, SA + q4, A_ + q4, B_ + q4);
-    uint16_t idx[S];
-#pragma unroll
-    for (int q8 = 0; q8 < S; q8 += 8) {
-      const uint4 v = __ldg(reinterpret_cast<const uint4*>(pt + base + q8));
-      const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        idx[q8 + 2 * t] = static_cast<uint16_t>(w4[t] & 0xffffu);
-        idx[q8 + 2 * t + 1] = static_cast<uint16_t>(w4[t] >> 16);
-      }
-    }
+    const Raw4 r = r_n;
+    const uint2 iv = i_n;
     float Al[S][8];
-    ck.load(j, Al[0]);
+#pragma unroll
+    for (int s = 0; s < 8; ++s) Al[0][s] = c_n[s];
+    if (j > 0) {
+      r_n = load_raw4(sys, apr, par, base - S);
+      i_n = __ldg(reinterpret_cast<const uint2*>(pt + base - S));
+      ck.load(j - 1, c_n);
+    }
+    float SA[S], A_[S], B_[S];
+    scale4(r, SA, A_, B_);
 #pragma unroll
     for (int t = 0; t + 1 < S; ++t) {
 #pragma unroll
       for (int s = 0; s < 8; ++s) Al[t + 1][s] = Al[t][s];
       alpha_step(Al[t + 1], A_[t], B_[t]);
     }
+    const uint32_t w2[2] = {iv.x, iv.y};
 #pragma unroll
     for (int t = S - 1; t >= 0; --t) {
       const float e = io.scale * (kLn2 * extrinsic2(Al[t], be, B_[t]));
-      const int n = idx[t];
+      const int n = static_cast<int>((w2[t >> 1] >> (16 * (t & 1))) & 0xffffu);
       io.ext[cb.work + n] = e;
-      if (LOWER) io.post[cb.out + n] = SA[t] + e;
+      if (POST) io.post[cb.out + n] = SA[t] + e;
       beta_step(be, A_[t], B_[t]);
       if (rec_beta && base + t == lo + G) {
         bseed[0] = make_float4(be[0], be[1], be[2], be[3]);

@@ -64,8 +64,9 @@ __device__ __forceinline__ void alpha_step(float (&al)[8], float a, float b) {
                      al[p0 + 1] + branch(u, n2 ^ n1 ^ 1, g0, g1));
   }
   const float r = an[0];
+  al[0] = 0.0f;  // an[0] - an[0]
 #pragma unroll
-  for (int s = 0; s < 8; ++s) al[s] = an[s] - r;
+  for (int s = 1; s < 8; ++s) al[s] = an[s] - r;
 }
 
 // beta_t from beta_{t+1} (in place); normalised so that state 0 is 0.
@@ -77,8 +78,9 @@ __device__ __forceinline__ void beta_step(float (&be)[8], float a, float b) {
     bn[s] = max_star(be[next_state(s, 0)] + branch(0, parity(s, 0), g0, g1),
                      be[next_state(s, 1)] + branch(1, parity(s, 1), g0, g1));
   const float r = bn[0];
+  be[0] = 0.0f;  // bn[0] - bn[0]
 #pragma unroll
-  for (int s = 0; s < 8; ++s) be[s] = bn[s] - r;
+  for (int s = 1; s < 8; ++s) be[s] = bn[s] - r;
 }
 
 // Extrinsic LLR (base-2) of one step: log-sum over the u=1 branches minus log-sum over the
@@ -124,7 +126,8 @@ __device__ __forceinline__ void tail_beta(float (&be)[8], const float ts[3], con
   }
   const float r = be[0];
 #pragma unroll
-  for (int s = 0; s < 8; ++s) be[s] -= r;
+  for (int s = 1; s < 8; ++s) be[s] -= r;
+  be[0] = 0.0f;
 }
 
 __device__ __forceinline__ void alpha_start(float (&al)[8]) {
