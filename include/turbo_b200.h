@@ -132,6 +132,26 @@ TC_API int tc_decode(tc_decoder* dec, size_t n_cb, const tc_code_block* cbs, siz
               const float* llr, size_t post_len, float* posterior, uint8_t* crc_ok,
               uint32_t* iterations_used, const tc_decode_options* opts);
 
+/* ---------------- decoding without device allocation ----------------
+ * No counterpart in the reference.  The same plain-schedule decode as tc_decode with
+ * TC_MEM_DEVICE, for callers that must not allocate device memory: a real-time receiver thread
+ * that cannot absorb the synchronisation and latency of cudaMalloc/cudaFree, a program whose
+ * device memory belongs to another allocator, a plug-in handed only its input and output
+ * buffers.  No decoder object is needed; it runs on the current device, ordered on
+ * opts->stream (NULL = the legacy default stream), and returns once enqueued.  llr, posterior,
+ * crc_ok and iterations_used are device pointers (the last two may be NULL).
+ *
+ * Every other device buffer comes from a fixed 32 MiB array compiled into the library (held on
+ * each GPU that loads it until the library is unloaded); a request that needs more is refused
+ * with TC_ERR_CAPACITY before any work is enqueued (*scratch_bytes, when given, receives the
+ * bytes the request needs; about 135 KB per K=6144 code block, i.e. ~240 such blocks).  The
+ * first call on a device copies constant tables synchronously: make it before capturing a
+ * stream.  All calls on a device share the array; calls that overlap on the GPU race. */
+TC_API int tc_decode_noalloc(size_t n_cb, const tc_code_block* cbs, size_t llr_len,
+                             const float* llr, size_t post_len, float* posterior,
+                             uint8_t* crc_ok, uint32_t* iterations_used,
+                             const tc_decode_options* opts, size_t* scratch_bytes);
+
 /* ---------------- kernel accounting (new) ----------------
  * Every kernel launch is counted.  With timing on, each SISO half-iteration launch is
  * bracketed by CUDA events on its launching stream; tc_decoder_timing waits for those events

@@ -113,6 +113,7 @@ _SIGNATURES = {
     "tc_decoder_destroy": [_VP],
     "tc_decode_options_init": [_VP],
     "tc_decode": [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, _VP, _VP, _VP],
+    "tc_decode_noalloc": [_SZ, _VP, _SZ, _VP, _SZ, _VP, _VP, _VP, _VP, _VP],
     "tc_decoder_set_timing": [_VP, C.c_int],
     "tc_decoder_timing": [_VP, _VP, C.c_int],
 }

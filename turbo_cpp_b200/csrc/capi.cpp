@@ -282,6 +282,35 @@ int tc_decode(tc_decoder* dec, size_t n_cb, const tc_code_block* cbs, size_t llr
   });
 }
 
+int tc_decode_noalloc(size_t n_cb, const tc_code_block* cbs, size_t llr_len, const float* llr,
+                      size_t post_len, float* posterior, uint8_t* crc_ok,
+                      uint32_t* iterations_used, const tc_decode_options* opts,
+                      size_t* scratch_bytes) {
+  return guarded([&] {
+    need(n_cb == 0 || (cbs && llr && posterior), "null pointer");
+    tc_decode_options o;
+    if (opts) o = *opts; else tc_decode_options_init(&o);
+    need(o.max_iterations <= 64, "max_iterations above 64");
+    tcb::DecodeRequest rq;
+    rq.n_cb = n_cb;
+    rq.cbs = reinterpret_cast<const tcb::CodeBlockDesc*>(cbs);
+    rq.llr_len = llr_len;
+    rq.llr = llr;
+    rq.post_len = post_len;
+    rq.posterior = posterior;
+    rq.crc_ok = crc_ok;
+    rq.iterations_used = iterations_used;
+    rq.max_iterations = o.max_iterations;
+    rq.early_stop = o.early_stop != 0;
+    rq.window = o.window;
+    rq.guard = o.guard;
+    rq.device_memory = true;
+    rq.scales = o.scales;
+    rq.stream = o.stream;
+    tcb::decode_noalloc(rq, scratch_bytes);
+  });
+}
+
 int tc_decoder_set_timing(tc_decoder* dec, int enable) {
   return guarded([&] {
     need(dec != nullptr, "null decoder");

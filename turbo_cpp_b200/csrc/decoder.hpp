@@ -116,4 +116,10 @@ class Decoder {
       d_done_, d_iters_, d_crc_, d_ckpt_;
 };
 
+// Plain-schedule decode on the current device with all scratch in a fixed array of the library
+// image (noalloc.cu); device pointers in rq, ordered on rq.stream; never allocates.  Writes the
+// scratch bytes the request needs to *bytes_needed when given, and throws CapacityExceeded when
+// they exceed the array.
+void decode_noalloc(const DecodeRequest& rq, size_t* bytes_needed);
+
 }  // namespace tcb
