@@ -125,6 +125,11 @@ typedef struct {
 
 TC_API int tc_decode_options_init(tc_decode_options* opts);
 
+/* Waits until the work this decoder has enqueued is done.  Returns TC_ERR_TIMEOUT (once) when a
+ * persistent-schedule wait on the device gave up since the last check; host-memory calls report
+ * that themselves, device-memory callers learn it here. */
+TC_API int tc_decoder_sync(tc_decoder* dec);
+
 /* Decodes n_cb code blocks.  llr has llr_len floats, posterior post_len floats; crc_ok
  * (n_cb bytes) and iterations_used (n_cb words) may be NULL.  With TC_MEM_HOST the call is
  * synchronous; with TC_MEM_DEVICE it is ordered on opts->stream and returns once enqueued. */

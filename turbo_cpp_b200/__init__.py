@@ -114,6 +114,7 @@ _SIGNATURES = {
     "tc_decode_options_init": [_VP],
     "tc_decode": [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, _VP, _VP, _VP],
     "tc_decode_noalloc": [_SZ, _VP, _SZ, _VP, _SZ, _VP, _VP, _VP, _VP, _VP],
+    "tc_decoder_sync": [_VP],
     "tc_decoder_set_timing": [_VP, C.c_int],
     "tc_decoder_timing": [_VP, _VP, C.c_int],
 }
@@ -483,6 +484,10 @@ class Decoder:
             opt.scales = keep.ctypes.data
         opt.stream = stream or None
         return opt, keep
+
+    def sync(self) -> None:
+        """Waits for enqueued work; raises DeviceTimeout if a device-side wait gave up."""
+        _call("tc_decoder_sync", self._h)
 
     def set_timing(self, on: bool) -> None:
         _call("tc_decoder_set_timing", self._h, int(bool(on)))

@@ -276,6 +276,7 @@ int tc_decode(tc_decoder* dec, size_t n_cb, const tc_code_block* cbs, size_t llr
     rq.window = o.window;
     rq.guard = o.guard;
     rq.device_memory = o.memory == TC_MEM_DEVICE;
+    rq.persistent = o.schedule == TC_SCHEDULE_PERSISTENT;
     rq.scales = o.scales;
     rq.stream = o.stream;
     dec->impl.decode(rq);
@@ -308,6 +309,13 @@ int tc_decode_noalloc(size_t n_cb, const tc_code_block* cbs, size_t llr_len, con
     rq.scales = o.scales;
     rq.stream = o.stream;
     tcb::decode_noalloc(rq, scratch_bytes);
+  });
+}
+
+int tc_decoder_sync(tc_decoder* dec) {
+  return guarded([&] {
+    need(dec != nullptr, "null decoder");
+    dec->impl.sync();
   });
 }
 

@@ -7,6 +7,7 @@
 
 #include <cstdint>
 
+#include "decoder.hpp"
 #include "siso.cuh"
 
 namespace tcb {
@@ -94,6 +95,128 @@ __global__ void finish_kernel(int n_cb, const uint8_t* __restrict__ done, uint8_
                               int early_stop) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n_cb) crc_ok[i] = early_stop ? done[i] : 0;
+}
+
+// ------------------------------------------------------------------------------------------
+// Persistent schedule: one launch for all iterations, fed by a device work queue.  A task is up
+// to 32 windows (one per lane) of one or more whole code blocks; a work item is one SISO
+// half-iteration of one task.  Items are handed out in half-iteration order (all tasks' first
+// half, then all tasks' second half, ...), so the item a warp waits for -- the same task's
+// previous half -- was always handed out earlier to a running warp.  Progress per task is a
+// counter released with a fence after the half's stores; a warp that waits longer than
+// kSpinLimit polls sets the error flag and proceeds, so the kernel always terminates.  Blocks
+// whose CRC24B passes are skipped by every later item.
+// ------------------------------------------------------------------------------------------
+constexpr int kPersistThreads = 64;
+constexpr int kPersistMinBlocks = 8;
+constexpr int kMaxIterations = 64;
+constexpr unsigned kSpinLimit = 1u << 24;  // polls of ~64 ns: about a second
+
+struct PersistArgs {
+  const DevCb* cbs;
+  const int32_t* win_cb;
+  const int32_t* tasks;  // [n_tasks][32] launch-wide window index per lane, -1 = idle lane
+  int n_tasks;
+  int* queue;            // next work item (atomic), zero before the launch
+  int* progress;         // per task: half-iterations completed, zero before the launch
+  int* error;            // set when a wait gave up
+  const float* llr;
+  float* sys_i;
+  float* e1i;
+  float* e2;
+  float* post;
+  const uint16_t* perm;
+  const uint16_t* inv;
+  float* seed_up[2];
+  float* seed_lo[2];
+  float4* ckpt;
+  int ckpt_per_window;
+  int guard;
+  int max_iterations;
+  int early_stop;
+  uint8_t* done;
+  uint32_t* iters;
+  const uint32_t* xpow;
+  float scale[2 * kMaxIterations];
+};
+
+__device__ __forceinline__ int load_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void store_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__global__ void __launch_bounds__(kPersistThreads, kPersistMinBlocks)
+    persistent_kernel(const PersistArgs p) {
+  __shared__ uint32_t syn[kPersistThreads];
+  const int lane = threadIdx.x & 31;
+  const int wbase = threadIdx.x & ~31;
+  const int total = p.n_tasks * 2 * p.max_iterations;
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(p.queue, 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= total) break;
+    const int h = item / p.n_tasks;  // half-iteration index
+    const int t = item - h * p.n_tasks;
+    const int it = h >> 1, half = h & 1;
+    if (h > 0 && lane == 0) {  // wait until this task has completed half h-1
+      unsigned polls = 0;
+      while (load_acquire(p.progress + t) < h) {
+        if (++polls > kSpinLimit) {
+          atomicExch(p.error, 1);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __syncwarp();
+    __threadfence();  // order this lane's reads after lane 0's acquire
+    const int g = p.tasks[32 * t + lane];
+    const int c = g >= 0 ? p.win_cb[g] : -1;
+    DevCb cb{};
+    if (c >= 0) cb = p.cbs[c];
+    const int w = g - cb.win0;
+    const bool active = c >= 0 && __ldcg(p.done + c) == 0;
+    if (__any_sync(0xffffffffu, active)) {
+      const CkptGlobal ck{p.ckpt + static_cast<int64_t>(2) * p.ckpt_per_window * (g < 0 ? 0 : g)};
+      const bool post_now = p.early_stop || it + 1 == p.max_iterations;
+      const SisoIo io =
+          half == 0 ? SisoIo{p.llr, p.sys_i, p.e2, p.e1i, nullptr, p.perm, p.inv, p.seed_up[it & 1],
+                             p.seed_up[(it + 1) & 1], p.scale[2 * it], p.guard}
+                    : SisoIo{p.llr, p.sys_i, p.e1i, p.e2, p.post, p.perm, p.inv, p.seed_lo[it & 1],
+                             p.seed_lo[(it + 1) & 1], p.scale[2 * it + 1], p.guard};
+      if (active)
+        siso_window_rt<kSub, CkptGlobal, true>(cb, w, g, io, ck, half == 1, half == 1 && post_now);
+      if (half == 1 && p.early_stop) {
+        // CRC24B syndrome of the hard decisions (lte_turbo.cpp:792-804): each lane XORs
+        // x^(N-1-i) mod g over the set bits of its window, the block's first lane combines.
+        __threadfence();  // this lane's posterior stores, before the other lanes read them
+        __syncwarp();
+        uint32_t part = 0;
+        if (active) {
+          const int lo_p = w * cb.window, hi_p = min(lo_p + cb.window, cb.k);
+          const int n = cb.k - cb.filler;
+          for (int q = max(lo_p, cb.filler); q < hi_p; ++q)
+            if (__ldcg(p.post + cb.out + q) >= 0.0f) part ^= p.xpow[n - 1 - (q - cb.filler)];
+        }
+        syn[threadIdx.x] = part;
+        __syncwarp();
+        if (active && w == 0) {
+          uint32_t x = 0;
+          for (int j = 0; j < cb.nwin; ++j) x ^= syn[wbase + lane + j];
+          p.iters[c] = static_cast<uint32_t>(it + 1);
+          if (x == 0) p.done[c] = 1;
+        }
+      }
+    }
+    __threadfence();  // every lane's stores of this half-iteration, before the release
+    __syncwarp();
+    if (lane == 0) store_release(p.progress + t, h + 1);
+  }
 }
 
 }  // namespace

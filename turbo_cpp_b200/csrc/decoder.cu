@@ -99,6 +99,8 @@ Decoder::Decoder(int device) : device_(device) {
   check(cudaMemcpy(d_perm_.ptr, perm.data(), perm.size() * 2, cudaMemcpyHostToDevice), "upload perm");
   check(cudaMemcpy(d_inv_.ptr, inv.data(), inv.size() * 2, cudaMemcpyHostToDevice), "upload inv");
   check(cudaMemcpy(d_xpow_.ptr, xpow.data(), xpow.size() * 4, cudaMemcpyHostToDevice), "upload crc");
+  d_err_.reserve(sizeof(int));
+  check(cudaMemset(d_err_.ptr, 0, sizeof(int)), "zero error word");
 
   const int smem = smem_optin_;
   check(cudaFuncSetAttribute(siso_plain_kernel<kSub, 0, false>,
@@ -112,10 +114,17 @@ Decoder::Decoder(int device) : device_(device) {
                         reinterpret_cast<const void*>(siso_plain_kernel<kSub, 2, true>)})
     check(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 0),
           "carveout attr");
+  check(cudaFuncSetAttribute(persistent_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 0),
+        "carveout attr");
+  check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&persist_blocks_per_sm_, persistent_kernel,
+                                                      kPersistThreads, 0),
+        "occupancy");
 }
 
 Decoder::~Decoder() {
   cudaSetDevice(device_);
+  if (last_event_) cudaEventDestroy(static_cast<cudaEvent_t>(last_event_));
+  d_err_.release();
   for (auto& e : events_) {
     if (e.start) cudaEventDestroy(static_cast<cudaEvent_t>(e.start));
     if (e.stop) cudaEventDestroy(static_cast<cudaEvent_t>(e.stop));
@@ -125,6 +134,39 @@ Decoder::~Decoder() {
                           &d_sysi_, &d_e1i_, &d_e2_, &d_post_, &d_seed_, &d_done_, &d_iters_,
                           &d_crc_, &d_ckpt_})
     b->release();
+}
+
+void Decoder::order_after_previous(void* stream) {
+  if (last_event_)
+    check(cudaStreamWaitEvent(static_cast<cudaStream_t>(stream),
+                              static_cast<cudaEvent_t>(last_event_), 0), "cudaStreamWaitEvent");
+}
+
+void Decoder::mark_done(void* stream) {
+  if (!last_event_) {
+    cudaEvent_t e;
+    check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    last_event_ = e;
+  }
+  check(cudaEventRecord(static_cast<cudaEvent_t>(last_event_), static_cast<cudaStream_t>(stream)),
+        "cudaEventRecord");
+}
+
+void Decoder::take_error() {
+  int err = 0;
+  check(cudaMemcpy(&err, d_err_.ptr, sizeof(int), cudaMemcpyDeviceToHost), "read error word");
+  if (err != 0) {
+    check(cudaMemset(d_err_.ptr, 0, sizeof(int)), "clear error word");
+    throw DeviceTimeout("a persistent-schedule wait gave up (device queue stalled)");
+  }
+}
+
+void Decoder::sync() {
+  std::lock_guard<std::mutex> lock(mu_);
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  if (last_event_)
+    check(cudaEventSynchronize(static_cast<cudaEvent_t>(last_event_)), "cudaEventSynchronize");
+  take_error();
 }
 
 void Decoder::set_timing(bool on) {
@@ -179,6 +221,10 @@ int Decoder::pick_window(int32_t k, int32_t requested) const {
 }
 
 void Decoder::decode(const DecodeRequest& rq) {
+  if (rq.persistent) {
+    decode_persistent(rq);
+    return;
+  }
   std::lock_guard<std::mutex> lock(mu_);
   check(cudaSetDevice(device_), "cudaSetDevice");
   // device memory: the caller's stream as given (NULL = legacy default stream, as in CUDA);
@@ -191,6 +237,7 @@ void Decoder::decode(const DecodeRequest& rq) {
   // ---- validate and lay out ----
   if (reinterpret_cast<uintptr_t>(rq.llr) % 16 != 0)
     throw InvalidArgument("the LLR buffer must be 16-byte aligned");
+  order_after_previous(st);
   const int guard = rq.guard < 0 ? kDefaultGuard : rq.guard;
   if (guard % kGroup != 0) throw InvalidArgument("guard must be a multiple of 8");
   std::vector<DevCb> cbs(n);
@@ -325,7 +372,183 @@ void Decoder::decode(const DecodeRequest& rq) {
     if (rq.crc_ok) check(cudaMemcpyAsync(rq.crc_ok, crc, n, cudaMemcpyDeviceToHost, st), "copy crc out");
     if (rq.iterations_used)
       check(cudaMemcpyAsync(rq.iterations_used, iters, n * 4, cudaMemcpyDeviceToHost, st), "copy iters out");
+  }
+  mark_done(st);
+  if (!rq.device_memory) check(cudaStreamSynchronize(st), "sync");
+}
+
+// ------------------------------------------------------------------------------------------
+// Persistent schedule: warp tasks of whole code blocks, one launch for all iterations.
+// ------------------------------------------------------------------------------------------
+void Decoder::decode_persistent(const DecodeRequest& rq) {
+  std::lock_guard<std::mutex> lock(mu_);
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  cudaStream_t st = static_cast<cudaStream_t>(rq.device_memory ? rq.stream
+                                                               : (rq.stream ? rq.stream : stream_));
+  const size_t n = rq.n_cb;
+  if (n == 0) return;
+  if (reinterpret_cast<uintptr_t>(rq.llr) % 16 != 0)
+    throw InvalidArgument("the LLR buffer must be 16-byte aligned");
+  order_after_previous(st);
+  if (rq.max_iterations > static_cast<uint32_t>(kMaxIterations))
+    throw InvalidArgument("max_iterations above 64");
+  const int guard = rq.guard < 0 ? kDefaultGuard : rq.guard;
+  if (guard % kGroup != 0) throw InvalidArgument("guard must be a multiple of 8");
+  const int target = rq.window > 0 ? rq.window : kPersistWindow;
+
+  // ---- per block: at most 32 windows of >= `target` steps (a multiple of 8, >= guard) ----
+  std::vector<DevCb> cbs(n);
+  std::vector<int64_t> start(n);
+  int64_t work = 0;
+  int max_ckpt = 0;
+  for (size_t i = 0; i < n; ++i) {
+    const int32_t k = rq.cbs[i].k;
+    const int qi = qpp_index(k);
+    if (qi < 0) throw OutOfRange("unsupported QPP block size");
+    if (rq.cbs[i].filler < 0 || rq.cbs[i].filler >= k) throw InvalidArgument("invalid filler count");
+    if (rq.cbs[i].llr_offset < 0 || rq.cbs[i].llr_offset % 4 != 0 ||
+        static_cast<size_t>(rq.cbs[i].llr_offset) + 3 * static_cast<size_t>(k + 4) > rq.llr_len)
+      throw InvalidArgument("invalid LLR offset (must be a multiple of 4 and in range)");
+    if (rq.cbs[i].out_offset < 0 ||
+        static_cast<size_t>(rq.cbs[i].out_offset) + static_cast<size_t>(k) > rq.post_len)
+      throw InvalidArgument("invalid posterior offset");
+    DevCb& d = cbs[i];
+    d.k = k;
+    d.filler = rq.cbs[i].filler;
+    d.tab = tab_offset_[qi];
+    int nwin = std::max(1, std::min(32, k / std::max(target, 8)));
+    int wlen = ((k + nwin - 1) / nwin + kGroup - 1) / kGroup * kGroup;
+    if (nwin > 1 && wlen < guard) {  // windows may not be shorter than the guard
+      nwin = std::max(1, k / guard);
+      wlen = ((k + nwin - 1) / nwin + kGroup - 1) / kGroup * kGroup;
+    }
+    d.window = std::min<int32_t>(wlen, k);
+    d.nwin = (k + d.window - 1) / d.window;
+    d.llr = rq.cbs[i].llr_offset;
+    d.work = work;
+    d.out = rq.cbs[i].out_offset;
+    start[i] = work;
+    work += k;
+    max_ckpt = std::max(max_ckpt, d.window / kSub);
+  }
+  // ---- tasks: blocks sorted by size, largest first, packed first-fit into 32 lanes ----
+  std::vector<int32_t> order(n);
+  for (size_t i = 0; i < n; ++i) order[i] = static_cast<int32_t>(i);
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+    return cbs[a].nwin != cbs[b].nwin ? cbs[a].nwin > cbs[b].nwin : cbs[a].k > cbs[b].k;
+  });
+  std::vector<int32_t> wincb, tasks;
+  int lanes_used = 32;
+  for (const int32_t i : order) {
+    DevCb& d = cbs[i];
+    if (lanes_used + d.nwin > 32) {  // open a new task
+      tasks.insert(tasks.end(), 32, -1);
+      lanes_used = 0;
+    }
+    d.win0 = static_cast<int32_t>(wincb.size());
+    for (int w = 0; w < d.nwin; ++w) {
+      tasks[tasks.size() - 32 + lanes_used + w] = static_cast<int32_t>(wincb.size());
+      wincb.push_back(i);
+    }
+    lanes_used += d.nwin;
+  }
+  const int n_tasks = static_cast<int>(tasks.size() / 32);
+  const int n_win = static_cast<int>(wincb.size());
+
+  // ---- device buffers ----
+  DevCb* dcbs = grow<DevCb>(d_cbs_, n);
+  int32_t* dwin = grow<int32_t>(d_wincb_, n_win);
+  int64_t* dstart = grow<int64_t>(d_start_, n);
+  int32_t* dtasks = grow<int32_t>(d_tasks_, tasks.size());
+  int* dqueue = grow<int>(d_queue_, 2 + static_cast<size_t>(n_tasks));  // queue, error, progress
+  float* sysi = grow<float>(d_sysi_, work);
+  float* e1i = grow<float>(d_e1i_, work);
+  float* e2 = grow<float>(d_e2_, work);
+  float* seeds = grow<float>(d_seed_, static_cast<size_t>(n_win) * 16 * 4);
+  float4* ckpt = grow<float4>(d_ckpt_, static_cast<size_t>(n_win) * 2 * max_ckpt);
+  uint8_t* done = grow<uint8_t>(d_done_, n);
+  uint32_t* iters = (rq.device_memory && rq.iterations_used) ? rq.iterations_used
+                                                              : grow<uint32_t>(d_iters_, n);
+  uint8_t* crc = (rq.device_memory && rq.crc_ok) ? rq.crc_ok : grow<uint8_t>(d_crc_, n);
+  const float* llr = rq.llr;
+  float* post = rq.posterior;
+  if (!rq.device_memory) {
+    float* dl = grow<float>(d_llr_, rq.llr_len);
+    check(cudaMemcpyAsync(dl, rq.llr, rq.llr_len * sizeof(float), cudaMemcpyHostToDevice, st),
+          "copy LLRs in");
+    llr = dl;
+    post = grow<float>(d_post_, rq.post_len);
+    check(cudaMemsetAsync(post, 0, rq.post_len * sizeof(float), st), "zero posterior");
+  }
+  check(cudaMemcpyAsync(dcbs, cbs.data(), n * sizeof(DevCb), cudaMemcpyHostToDevice, st), "copy cbs");
+  check(cudaMemcpyAsync(dwin, wincb.data(), n_win * sizeof(int32_t), cudaMemcpyHostToDevice, st),
+        "copy windows");
+  check(cudaMemcpyAsync(dstart, start.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, st),
+        "copy starts");
+  check(cudaMemcpyAsync(dtasks, tasks.data(), tasks.size() * sizeof(int32_t),
+                        cudaMemcpyHostToDevice, st), "copy tasks");
+  check(cudaMemsetAsync(dqueue, 0, (2 + static_cast<size_t>(n_tasks)) * sizeof(int), st),
+        "zero queue");
+  check(cudaMemsetAsync(seeds, 0, static_cast<size_t>(n_win) * 16 * 4 * sizeof(float), st),
+        "zero seeds");
+  init_flags_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(
+      static_cast<int>(n), done, iters, rq.max_iterations);
+  setup_kernel<<<static_cast<unsigned>((work + 255) / 256), 256, 0, st>>>(
+      dcbs, dstart, static_cast<int>(n), work, llr, static_cast<const uint16_t*>(d_perm_.ptr),
+      sysi, e2);
+  check(cudaGetLastError(), "set-up launch");
+
+  PersistArgs a{};
+  a.cbs = dcbs;
+  a.win_cb = dwin;
+  a.tasks = dtasks;
+  a.n_tasks = n_tasks;
+  a.queue = dqueue;
+  a.error = static_cast<int*>(d_err_.ptr);
+  a.progress = dqueue + 2;
+  a.llr = llr;
+  a.sys_i = sysi;
+  a.e1i = e1i;
+  a.e2 = e2;
+  a.post = post;
+  a.perm = static_cast<const uint16_t*>(d_perm_.ptr);
+  a.inv = static_cast<const uint16_t*>(d_inv_.ptr);
+  const size_t slab = static_cast<size_t>(n_win) * 16;
+  a.seed_up[0] = seeds;
+  a.seed_up[1] = seeds + slab;
+  a.seed_lo[0] = seeds + 2 * slab;
+  a.seed_lo[1] = seeds + 3 * slab;
+  a.ckpt = ckpt;
+  a.ckpt_per_window = max_ckpt;
+  a.guard = guard;
+  a.max_iterations = static_cast<int>(rq.max_iterations);
+  a.early_stop = rq.early_stop ? 1 : 0;
+  a.done = done;
+  a.iters = iters;
+  a.xpow = static_cast<const uint32_t*>(d_xpow_.ptr);
+  for (int i = 0; i < 2 * kMaxIterations; ++i)
+    a.scale[i] = (rq.scales && i < 2 * static_cast<int>(rq.max_iterations)) ? rq.scales[i] : 1.0f;
+  const int grid = std::max(1, sm_count_ * std::max(persist_blocks_per_sm_, 1));
+  record_start(st);
+  persistent_kernel<<<grid, kPersistThreads, 0, st>>>(a);
+  check(cudaGetLastError(), "persistent launch");
+  record_stop(st, static_cast<uint64_t>(work) * 2 * rq.max_iterations);
+  finish_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(static_cast<int>(n), done,
+                                                                         crc, rq.early_stop ? 1 : 0);
+  check(cudaGetLastError(), "finish launch");
+  timing_.launches += 4;
+  if (!rq.device_memory) {
+    check(cudaMemcpyAsync(rq.posterior, post, rq.post_len * sizeof(float), cudaMemcpyDeviceToHost, st),
+          "copy posterior out");
+    if (rq.crc_ok) check(cudaMemcpyAsync(rq.crc_ok, crc, n, cudaMemcpyDeviceToHost, st), "copy crc out");
+    if (rq.iterations_used)
+      check(cudaMemcpyAsync(rq.iterations_used, iters, n * 4, cudaMemcpyDeviceToHost, st),
+            "copy iters out");
+    mark_done(st);
     check(cudaStreamSynchronize(st), "sync");
+    take_error();
+  } else {
+    mark_done(st);
   }
 }
 

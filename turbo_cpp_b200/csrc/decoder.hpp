@@ -34,6 +34,7 @@ constexpr int kSub = 4;              // alpha checkpoint interval (steps)
 constexpr int kGroup = 8;            // load granularity: windows and guards are multiples of 8
 constexpr int kDefaultWindow = 128;  // window length (steps)
 constexpr int kDefaultGuard = 96;    // warm-up steps on each side of a window
+constexpr int kPersistWindow = 192;  // target window of the persistent schedule (<= 32 per block)
 
 struct CodeBlockDesc {
   int32_t k;
@@ -57,6 +58,7 @@ struct DecodeRequest {
   int guard = -1;   // <0: default
   bool device_memory = false;  // llr/posterior/crc_ok/iterations_used are device pointers
   bool smem_checkpoints = false;  // alpha checkpoints in shared memory instead of global scratch
+  bool persistent = false;  // persistent warp-task schedule instead of per-half-iteration launches
   const float* scales = nullptr;  // host; 2 per iteration (upper, lower); null = all 1
   void* stream = nullptr;
 };
@@ -84,14 +86,16 @@ class Decoder {
   Decoder(const Decoder&) = delete;
   Decoder& operator=(const Decoder&) = delete;
 
-  void decode(const DecodeRequest& rq);  // plain schedule
+  void decode(const DecodeRequest& rq);  // plain or persistent schedule
   int device() const { return device_; }
   void set_timing(bool on);
+  void sync();  // waits for this decoder's enqueued work; reports a persistent wait timeout
   Timing timing(bool reset);  // waits for the recorded events
   int sm_count() const { return sm_count_; }
 
  private:
   int pick_window(int32_t k, int32_t requested) const;
+  void decode_persistent(const DecodeRequest& rq);
   void record_start(void* stream);
   void record_stop(void* stream, uint64_t steps);
 
@@ -113,7 +117,13 @@ class Decoder {
   std::vector<int32_t> tab_offset_;
   DeviceBuffer d_perm_, d_inv_, d_xpow_;
   DeviceBuffer d_cbs_, d_wincb_, d_start_, d_llr_, d_sysi_, d_e1i_, d_e2_, d_post_, d_seed_,
-      d_done_, d_iters_, d_crc_, d_ckpt_;
+      d_done_, d_iters_, d_crc_, d_ckpt_, d_tasks_, d_queue_;
+  int persist_blocks_per_sm_ = 0;
+  DeviceBuffer d_err_;          // sticky: set by a persistent-schedule wait that gave up
+  void* last_event_ = nullptr;  // completion of the previous decode (orders workspace reuse)
+  void order_after_previous(void* stream);
+  void mark_done(void* stream);
+  void take_error();  // throws DeviceTimeout (and clears the flag) if it is set; host-synchronous
 };
 
 // Plain-schedule decode on the current device with all scratch in a fixed array of the library

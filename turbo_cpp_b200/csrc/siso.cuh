@@ -49,14 +49,32 @@ struct SisoIo {
 __device__ __forceinline__ float4 ld4(const float* p) {
   return __ldg(reinterpret_cast<const float4*>(p));
 }
+// Loads of data written earlier in the same kernel (persistent schedule): an ordinary
+// (coherent, L1-cacheable) global load, never the read-only non-coherent path.  The writer
+// releases and the reader acquires at GPU scope before these loads, which makes them see the
+// writes even when the writer ran on another SM.
+__device__ __forceinline__ float4 ld4_coherent(const float* p) {
+  float4 v;
+  asm volatile("ld.global.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "l"(p)
+               : "memory");
+  return v;
+}
+template <bool COHERENT>
+__device__ __forceinline__ float4 ld4_io(const float* p) {
+  return COHERENT ? ld4_coherent(p) : ld4(p);
+}
 
-// Raw inputs of 4 consecutive steps (one float4 per stream).
+// Raw inputs of 4 consecutive steps (one float4 per stream).  The a-priori stream is written
+// by the other SISO; COHERENT reads it through L2 (needed when both run in one kernel).
 struct Raw4 {
   float4 s, e, p;  // systematic, a-priori, parity
 };
+template <bool COHERENT = false>
 __device__ __forceinline__ Raw4 load_raw4(const float* sys, const float* apr, const float* par,
                                           int q) {
-  return Raw4{ld4(sys + q), ld4(apr + q), ld4(par + q)};
+  return Raw4{ld4(sys + q), ld4_io<COHERENT>(apr + q), ld4(par + q)};
 }
 // raw -> sys+apr (sa), a = c (sys+apr), b = c par with c = log2(e)/2
 __device__ __forceinline__ void scale4(const Raw4& r, float* sa, float* a, float* b) {
@@ -72,9 +90,10 @@ __device__ __forceinline__ void scale4(const Raw4& r, float* sa, float* a, float
 struct Raw8 {
   Raw4 lo, hi;
 };
+template <bool COHERENT = false>
 __device__ __forceinline__ Raw8 load_raw8(const float* sys, const float* apr, const float* par,
                                           int q) {
-  return Raw8{load_raw4(sys, apr, par, q), load_raw4(sys, apr, par, q + 4)};
+  return Raw8{load_raw4<COHERENT>(sys, apr, par, q), load_raw4<COHERENT>(sys, apr, par, q + 4)};
 }
 
 // Checkpoint storage, 8 floats per checkpoint as two float4.  Shared memory: thread-minor
@@ -105,11 +124,11 @@ struct CkptGlobal {
 };
 
 // Tail LLRs in the reference's decoder mapping (lte_turbo.cpp:758-773).
-template <bool LOWER>
-__device__ __forceinline__ void tail_llrs(const float* d0, int k, float ts[3], float tp[3]) {
+__device__ __forceinline__ void tail_llrs(bool lower, const float* d0, int k, float ts[3],
+                                          float tp[3]) {
   const float* d1 = d0 + (k + 4);
   const float* d2 = d1 + (k + 4);
-  if (!LOWER) {
+  if (!lower) {
     ts[0] = d0[k]; ts[1] = d0[k + 2]; ts[2] = 0.0f;
     tp[0] = d1[k]; tp[1] = d0[k + 1]; tp[2] = d1[k + 2];
   } else {
@@ -119,10 +138,14 @@ __device__ __forceinline__ void tail_llrs(const float* d0, int k, float ts[3], f
 }
 
 // Runs window w of block cb for one half-iteration.  g = launch-wide window index (seed slot).
-// POST (lower SISO only): also write the posterior Ls + e1 + e2 (last iteration, early stop).
-template <int S, bool LOWER, bool POST, class Ckpt>
-__device__ __forceinline__ void siso_window(const DevCb& cb, int w, int g, const SisoIo& io,
-                                            const Ckpt& ck) {
+// lower: the SISO over interleaved order; post (lower SISO only): also write the posterior
+// Ls + e1 + e2 (last iteration, early stop).  Both may be compile-time constants (the plain
+// kernels, one specialisation each) or run-time values (the persistent kernel, which keeps a
+// single copy of this code for both halves).  COHERENT: a-priori and seeds were written earlier
+// in the same kernel (persistent schedule).
+template <int S, class Ckpt, bool COHERENT>
+__device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, const SisoIo& io,
+                                               const Ckpt& ck, const bool LOWER, const bool POST) {
   static_assert(S == 4, "sub-windows are one float4 group of 4 steps");
   const int K = cb.k, W = cb.window, G = io.guard;
   const int lo = w * W, hi = min(lo + W, K);
@@ -140,14 +163,14 @@ __device__ __forceinline__ void siso_window(const DevCb& cb, int w, int g, const
     a_lo = 0;
     alpha_start(al);
   } else {
-    const float4 x = ld4(io.seed_in + 16 * g), y = ld4(io.seed_in + 16 * g + 4);
+    const float4 x = ld4_io<COHERENT>(io.seed_in + 16 * g), y = ld4_io<COHERENT>(io.seed_in + 16 * g + 4);
     al[0] = x.x; al[1] = x.y; al[2] = x.z; al[3] = x.w; al[4] = y.x; al[5] = y.y; al[6] = y.z; al[7] = y.w;
   }
   {  // 8-step groups (both halves of each sector); the next group is requested early
-    Raw8 cur = load_raw8(sys, apr, par, a_lo);
+    Raw8 cur = load_raw8<COHERENT>(sys, apr, par, a_lo);
     for (int q = a_lo; q < hi; q += 8) {
       Raw8 nxt = cur;
-      if (q + 8 < hi) nxt = load_raw8(sys, apr, par, q + 8);
+      if (q + 8 < hi) nxt = load_raw8<COHERENT>(sys, apr, par, q + 8);
       if (q >= lo) ck.store((q - lo) / S, al);
       scale4(cur.lo, sa, a, b);
 #pragma unroll
@@ -179,17 +202,17 @@ __device__ __forceinline__ void siso_window(const DevCb& cb, int w, int g, const
   if (b_hi >= K) {
     b_hi = K;
     float ts[3], tp[3];
-    tail_llrs<LOWER>(d0, K, ts, tp);
+    tail_llrs(LOWER, d0, K, ts, tp);
     tail_beta(be, ts, tp);
   } else {
-    const float4 x = ld4(io.seed_in + 16 * g + 8), y = ld4(io.seed_in + 16 * g + 12);
+    const float4 x = ld4_io<COHERENT>(io.seed_in + 16 * g + 8), y = ld4_io<COHERENT>(io.seed_in + 16 * g + 12);
     be[0] = x.x; be[1] = x.y; be[2] = x.z; be[3] = x.w; be[4] = y.x; be[5] = y.y; be[6] = y.z; be[7] = y.w;
   }
   if (b_hi > hi) {
-    Raw8 cur = load_raw8(sys, apr, par, b_hi - 8);
+    Raw8 cur = load_raw8<COHERENT>(sys, apr, par, b_hi - 8);
     for (int q = b_hi - 8; q >= hi; q -= 8) {
       Raw8 nxt = cur;
-      if (q - 8 >= hi) nxt = load_raw8(sys, apr, par, q - 8);
+      if (q - 8 >= hi) nxt = load_raw8<COHERENT>(sys, apr, par, q - 8);
       scale4(cur.hi, sa, a, b);
 #pragma unroll
       for (int t = 3; t >= 0; --t) beta_step(be, a[t], b[t]);
@@ -215,7 +238,7 @@ __device__ __forceinline__ void siso_window(const DevCb& cb, int w, int g, const
   float c_n[8];
   if (nsub > 0) {
     const int base = lo + (nsub - 1) * S;
-    r_n = load_raw4(sys, apr, par, base);
+    r_n = load_raw4<COHERENT>(sys, apr, par, base);
     i_n = __ldg(reinterpret_cast<const uint2*>(pt + base));
     ck.load(nsub - 1, c_n);
   }
@@ -227,7 +250,7 @@ __device__ __forceinline__ void siso_window(const DevCb& cb, int w, int g, const
 #pragma unroll
     for (int s = 0; s < 8; ++s) Al[0][s] = c_n[s];
     if (j > 0) {
-      r_n = load_raw4(sys, apr, par, base - S);
+      r_n = load_raw4<COHERENT>(sys, apr, par, base - S);
       i_n = __ldg(reinterpret_cast<const uint2*>(pt + base - S));
       ck.load(j - 1, c_n);
     }
@@ -253,6 +276,12 @@ __device__ __forceinline__ void siso_window(const DevCb& cb, int w, int g, const
       }
     }
   }
+}
+
+template <int S, bool LOWER, bool POST, class Ckpt, bool COHERENT = false>
+__device__ __forceinline__ void siso_window(const DevCb& cb, int w, int g, const SisoIo& io,
+                                            const Ckpt& ck) {
+  siso_window_rt<S, Ckpt, COHERENT>(cb, w, g, io, ck, LOWER, POST);
 }
 
 }  // namespace tcb
