@@ -109,7 +109,11 @@ typedef struct {
 } tc_code_block;
 
 enum { TC_MEM_HOST = 0, TC_MEM_DEVICE = 1 };
-enum { TC_SCHEDULE_PLAIN = 0, TC_SCHEDULE_PERSISTENT = 1 };
+/* PLAIN: one launch per SISO half-iteration over all blocks (host-driven iteration loop).
+ * PERSISTENT: one launch for all iterations, warps pull (task, half-iteration) items from a
+ * device queue, blocks stop individually on CRC24B.  AUTO: the schedule and window that
+ * tc_autotune found fastest for requests of the same signature (PLAIN, window 128 if none). */
+enum { TC_SCHEDULE_PLAIN = 0, TC_SCHEDULE_PERSISTENT = 1, TC_SCHEDULE_AUTO = 2 };
 
 typedef struct {
   uint32_t max_iterations; /* default 8                                                   */
@@ -119,16 +123,41 @@ typedef struct {
   uint32_t memory;         /* TC_MEM_HOST (synchronous, copies inside) or TC_MEM_DEVICE   */
   uint32_t schedule;       /* TC_SCHEDULE_PLAIN or TC_SCHEDULE_PERSISTENT                 */
   const float* scales;     /* host array, 2 per iteration (upper, lower); NULL = 1.0     */
+  uint32_t graph;          /* TC_MEM_DEVICE only: capture this request's launch sequence in a
+                              CUDA graph the first time and replay it when the same shapes,
+                              buffers and options come again (16 graphs kept per decoder)  */
   void* stream;            /* cudaStream_t; TC_MEM_DEVICE: used as given (NULL = the legacy
                               default stream); TC_MEM_HOST: NULL = the decoder's own stream */
 } tc_decode_options;
 
 TC_API int tc_decode_options_init(tc_decode_options* opts);
 
+/* Autotuning (new): decodes the given TC_MEM_DEVICE request with each candidate schedule and
+ * window length (plain 128..256, persistent 192..320; a few decodes each), keeps the fastest for
+ * requests of the same signature (early stop, iterations, block count and mean K, rounded) and
+ * reports it.  tc_autotune_save/load write and read the table as text. */
+typedef struct {
+  int32_t schedule; /* TC_SCHEDULE_PLAIN or TC_SCHEDULE_PERSISTENT */
+  int32_t window;
+  double ms;        /* time of one decode with that choice */
+} tc_tune_result;
+TC_API int tc_autotune(tc_decoder* dec, size_t n_cb, const tc_code_block* cbs, size_t llr_len,
+                       const float* llr, size_t post_len, float* posterior,
+                       const tc_decode_options* opts, tc_tune_result* best);
+TC_API int tc_autotune_save(tc_decoder* dec, const char* path);
+TC_API int tc_autotune_load(tc_decoder* dec, const char* path);
+
 /* Waits until the work this decoder has enqueued is done.  Returns TC_ERR_TIMEOUT (once) when a
  * persistent-schedule wait on the device gave up since the last check; host-memory calls report
  * that themselves, device-memory callers learn it here. */
 TC_API int tc_decoder_sync(tc_decoder* dec);
+
+/* Testing hook for the failure path (new): while set, persistent decodes on this decoder make
+ * the warps working on task `task` (the task queue's order: largest blocks first) wait for a
+ * progress count that is never reached.  The device-side wait limit (one second) runs out, the
+ * kernel still finishes, and the call reports TC_ERR_TIMEOUT (host memory) or tc_decoder_sync
+ * does (device memory); the results of that call are not valid.  -1 turns it off. */
+TC_API int tc_decoder_inject_stall(tc_decoder* dec, int task);
 
 /* Decodes n_cb code blocks.  llr has llr_len floats, posterior post_len floats; crc_ok
  * (n_cb bytes) and iterations_used (n_cb words) may be NULL.  With TC_MEM_HOST the call is

@@ -26,14 +26,14 @@ __all__ = [
     "encode_transport_block", "compute_e", "rate_match", "derate_match_code_block",
     "derate_match_llr", "random_bits", "awgn_llr", "awgn_code_blocks", "Decoder", "DecodeOptions",
     "turbo_decode_code_block_gpu", "decode_transport_block", "MEM_HOST", "MEM_DEVICE",
-    "SCHEDULE_PLAIN", "SCHEDULE_PERSISTENT",
+    "SCHEDULE_PLAIN", "SCHEDULE_PERSISTENT", "SCHEDULE_AUTO",
 ]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libturbo_b200.so")
 
 MEM_HOST, MEM_DEVICE = 0, 1
-SCHEDULE_PLAIN, SCHEDULE_PERSISTENT = 0, 1
+SCHEDULE_PLAIN, SCHEDULE_PERSISTENT, SCHEDULE_AUTO = 0, 1, 2
 
 
 # ------------------------------------------------------------------------------------------
@@ -79,7 +79,11 @@ class _CodeBlock(C.Structure):
 class _Options(C.Structure):
     _fields_ = [("max_iterations", C.c_uint32), ("early_stop", C.c_uint32), ("window", C.c_int32),
                 ("guard", C.c_int32), ("memory", C.c_uint32), ("schedule", C.c_uint32),
-                ("scales", C.c_void_p), ("stream", C.c_void_p)]
+                ("scales", C.c_void_p), ("graph", C.c_uint32), ("stream", C.c_void_p)]
+
+
+class _TuneResult(C.Structure):
+    _fields_ = [("schedule", C.c_int32), ("window", C.c_int32), ("ms", C.c_double)]
 
 
 class _Seg(C.Structure):
@@ -115,6 +119,10 @@ _SIGNATURES = {
     "tc_decode": [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, _VP, _VP, _VP],
     "tc_decode_noalloc": [_SZ, _VP, _SZ, _VP, _SZ, _VP, _VP, _VP, _VP, _VP],
     "tc_decoder_sync": [_VP],
+    "tc_decoder_inject_stall": [_VP, C.c_int],
+    "tc_autotune": [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, _VP, _VP],
+    "tc_autotune_save": [_VP, C.c_char_p],
+    "tc_autotune_load": [_VP, C.c_char_p],
     "tc_decoder_set_timing": [_VP, C.c_int],
     "tc_decoder_timing": [_VP, _VP, C.c_int],
 }
@@ -444,6 +452,7 @@ class DecodeOptions:
     guard: int = -1          # <0: default (96)
     schedule: int = SCHEDULE_PLAIN
     scales: Optional[Sequence[float]] = None  # 2 per iteration; None = 1.0
+    graph: bool = False      # device memory: capture once, replay the CUDA graph
 
 
 class Decoder:
@@ -482,12 +491,34 @@ class Decoder:
             if keep.size < 2 * o.max_iterations:
                 raise InvalidArgument("scales needs 2 entries per iteration")
             opt.scales = keep.ctypes.data
+        opt.graph = int(bool(o.graph))
         opt.stream = stream or None
         return opt, keep
+
+    def inject_stall(self, task: int) -> None:
+        """Testing hook: persistent decodes time out waiting on `task` (-1 turns it off)."""
+        _call("tc_decoder_inject_stall", self._h, int(task))
 
     def sync(self) -> None:
         """Waits for enqueued work; raises DeviceTimeout if a device-side wait gave up."""
         _call("tc_decoder_sync", self._h)
+
+    def autotune(self, cbs, n_cb: int, llr_ptr: int, llr_len: int, post_ptr: int, post_len: int,
+                 options: Optional[DecodeOptions] = None, stream: int = 0) -> dict:
+        """Times the candidate schedules/windows on this device-memory request and remembers the
+        fastest for SCHEDULE_AUTO; returns {schedule, window, ms}."""
+        o = options or DecodeOptions()
+        opt, _keep = self._opts(o, MEM_DEVICE, stream)
+        r = _TuneResult()
+        _call("tc_autotune", self._h, int(n_cb), C.addressof(cbs), int(llr_len), llr_ptr,
+              int(post_len), post_ptr, C.addressof(opt), C.addressof(r))
+        return {"schedule": r.schedule, "window": r.window, "ms": r.ms}
+
+    def save_tuning(self, path: str) -> None:
+        _call("tc_autotune_save", self._h, os.fsencode(path))
+
+    def load_tuning(self, path: str) -> None:
+        _call("tc_autotune_load", self._h, os.fsencode(path))
 
     def set_timing(self, on: bool) -> None:
         _call("tc_decoder_set_timing", self._h, int(bool(on)))

@@ -258,7 +258,8 @@ int tc_decode(tc_decoder* dec, size_t n_cb, const tc_code_block* cbs, size_t llr
     tc_decode_options o;
     if (opts) o = *opts; else tc_decode_options_init(&o);
     need(o.memory == TC_MEM_HOST || o.memory == TC_MEM_DEVICE, "unknown memory kind");
-    need(o.schedule == TC_SCHEDULE_PLAIN || o.schedule == TC_SCHEDULE_PERSISTENT,
+    need(o.schedule == TC_SCHEDULE_PLAIN || o.schedule == TC_SCHEDULE_PERSISTENT ||
+             o.schedule == TC_SCHEDULE_AUTO,
          "unknown schedule");
     need(o.max_iterations <= 64, "max_iterations above 64");
     static_assert(sizeof(tc_code_block) == sizeof(tcb::CodeBlockDesc), "descriptor layout");
@@ -277,6 +278,8 @@ int tc_decode(tc_decoder* dec, size_t n_cb, const tc_code_block* cbs, size_t llr
     rq.guard = o.guard;
     rq.device_memory = o.memory == TC_MEM_DEVICE;
     rq.persistent = o.schedule == TC_SCHEDULE_PERSISTENT;
+    rq.auto_schedule = o.schedule == TC_SCHEDULE_AUTO;
+    rq.graph = o.graph != 0;
     rq.scales = o.scales;
     rq.stream = o.stream;
     dec->impl.decode(rq);
@@ -309,6 +312,57 @@ int tc_decode_noalloc(size_t n_cb, const tc_code_block* cbs, size_t llr_len, con
     rq.scales = o.scales;
     rq.stream = o.stream;
     tcb::decode_noalloc(rq, scratch_bytes);
+  });
+}
+
+int tc_autotune(tc_decoder* dec, size_t n_cb, const tc_code_block* cbs, size_t llr_len,
+                const float* llr, size_t post_len, float* posterior,
+                const tc_decode_options* opts, tc_tune_result* best) {
+  return guarded([&] {
+    need(dec != nullptr && cbs && llr && posterior, "null pointer");
+    tc_decode_options o;
+    if (opts) o = *opts; else tc_decode_options_init(&o);
+    need(o.memory == TC_MEM_DEVICE, "autotuning needs TC_MEM_DEVICE buffers");
+    tcb::DecodeRequest rq;
+    rq.n_cb = n_cb;
+    rq.cbs = reinterpret_cast<const tcb::CodeBlockDesc*>(cbs);
+    rq.llr_len = llr_len;
+    rq.llr = llr;
+    rq.post_len = post_len;
+    rq.posterior = posterior;
+    rq.max_iterations = o.max_iterations;
+    rq.early_stop = o.early_stop != 0;
+    rq.guard = o.guard;
+    rq.device_memory = true;
+    rq.scales = o.scales;
+    rq.stream = o.stream;
+    const auto c = dec->impl.autotune(rq);
+    if (best) {
+      best->schedule = c.persistent ? TC_SCHEDULE_PERSISTENT : TC_SCHEDULE_PLAIN;
+      best->window = c.window;
+      best->ms = c.ms;
+    }
+  });
+}
+
+int tc_autotune_save(tc_decoder* dec, const char* path) {
+  return guarded([&] {
+    need(dec != nullptr && path != nullptr, "null pointer");
+    dec->impl.save_tuning(path);
+  });
+}
+
+int tc_autotune_load(tc_decoder* dec, const char* path) {
+  return guarded([&] {
+    need(dec != nullptr && path != nullptr, "null pointer");
+    dec->impl.load_tuning(path);
+  });
+}
+
+int tc_decoder_inject_stall(tc_decoder* dec, int task) {
+  return guarded([&] {
+    need(dec != nullptr, "null decoder");
+    dec->impl.inject_stall(task);
   });
 }
 

@@ -104,13 +104,13 @@ __global__ void finish_kernel(int n_cb, const uint8_t* __restrict__ done, uint8_
 // half, then all tasks' second half, ...), so the item a warp waits for -- the same task's
 // previous half -- was always handed out earlier to a running warp.  Progress per task is a
 // counter released with a fence after the half's stores; a warp that waits longer than
-// kSpinLimit polls sets the error flag and proceeds, so the kernel always terminates.  Blocks
-// whose CRC24B passes are skipped by every later item.
+// kWaitLimitNs (one second of the GPU global timer) sets the error flag and proceeds, so the
+// kernel always terminates.  Blocks whose CRC24B passes are skipped by every later item.
 // ------------------------------------------------------------------------------------------
 constexpr int kPersistThreads = 64;
 constexpr int kPersistMinBlocks = 8;
 constexpr int kMaxIterations = 64;
-constexpr unsigned kSpinLimit = 1u << 24;  // polls of ~64 ns: about a second
+constexpr uint64_t kWaitLimitNs = 1000000000ull;  // one second
 
 struct PersistArgs {
   const DevCb* cbs;
@@ -120,6 +120,7 @@ struct PersistArgs {
   int* queue;            // next work item (atomic), zero before the launch
   int* progress;         // per task: half-iterations completed, zero before the launch
   int* error;            // set when a wait gave up
+  int stall_task;        // testing hook: this task's waits are never satisfied (-1: off)
   const float* llr;
   float* sys_i;
   float* e1i;
@@ -145,6 +146,11 @@ __device__ __forceinline__ int load_acquire(const int* p) {
   asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 __device__ __forceinline__ void store_release(int* p, int v) {
   asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
@@ -164,13 +170,14 @@ __global__ void __launch_bounds__(kPersistThreads, kPersistMinBlocks)
     const int t = item - h * p.n_tasks;
     const int it = h >> 1, half = h & 1;
     if (h > 0 && lane == 0) {  // wait until this task has completed half h-1
-      unsigned polls = 0;
-      while (load_acquire(p.progress + t) < h) {
-        if (++polls > kSpinLimit) {
+      const int need = (t == p.stall_task) ? 0x7fffffff : h;
+      const uint64_t t0 = global_ns();
+      while (load_acquire(p.progress + t) < need) {
+        if (global_ns() - t0 > kWaitLimitNs) {
           atomicExch(p.error, 1);
           break;
         }
-        __nanosleep(64);
+        __nanosleep(256);
       }
     }
     __syncwarp();

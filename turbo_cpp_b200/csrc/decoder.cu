@@ -8,7 +8,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <sstream>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -27,13 +31,39 @@ void check(cudaError_t e, const char* what) {
     throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+}  // namespace
+
 template <class T>
-T* grow(DeviceBuffer& b, size_t count) {
+T* Decoder::grow(DeviceBuffer& b, size_t count) {
+  void* before = b.ptr;
   b.reserve(count * sizeof(T));
+  if (b.ptr != before) ++generation_;  // cached graphs hold the old addresses
   return static_cast<T*>(b.ptr);
 }
 
-}  // namespace
+void Decoder::upload(void* dst, const void* src, size_t bytes, void* stream) {
+  if (bytes == 0) return;
+  const size_t padded = (bytes + 255) & ~size_t{255};
+  upload_bytes_ += padded;
+  if (capturing_ != nullptr) {  // the graph reads its own pinned copy at every replay
+    GraphEntry& g = *capturing_;
+    if (g.arena_used + padded > g.arena_bytes)
+      throw CudaError("graph descriptor arena too small");
+    char* pinned = static_cast<char*>(g.arena) + g.arena_used;
+    g.arena_used += padded;
+    std::memcpy(pinned, src, bytes);
+    src = pinned;
+  }
+  check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, static_cast<cudaStream_t>(stream)),
+        "copy descriptors");
+}
+
+void Decoder::drop_graph(GraphEntry& e) {
+  if (e.exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(e.exec));
+  if (e.arena) cudaFreeHost(e.arena);
+  e.exec = nullptr;
+  e.arena = nullptr;
+}
 
 // ------------------------------------------------------------------------------------------
 void DeviceBuffer::reserve(size_t need) {
@@ -123,6 +153,7 @@ Decoder::Decoder(int device) : device_(device) {
 
 Decoder::~Decoder() {
   cudaSetDevice(device_);
+  for (auto& g : graphs_) drop_graph(g);
   if (last_event_) cudaEventDestroy(static_cast<cudaEvent_t>(last_event_));
   d_err_.release();
   for (auto& e : events_) {
@@ -137,12 +168,14 @@ Decoder::~Decoder() {
 }
 
 void Decoder::order_after_previous(void* stream) {
+  if (capturing_ != nullptr) return;  // a replayed graph is ordered at its launch
   if (last_event_)
     check(cudaStreamWaitEvent(static_cast<cudaStream_t>(stream),
                               static_cast<cudaEvent_t>(last_event_), 0), "cudaStreamWaitEvent");
 }
 
 void Decoder::mark_done(void* stream) {
+  if (capturing_ != nullptr) return;
   if (!last_event_) {
     cudaEvent_t e;
     check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
@@ -220,12 +253,216 @@ int Decoder::pick_window(int32_t k, int32_t requested) const {
   return std::min<int32_t>(kDefaultWindow, k);
 }
 
-void Decoder::decode(const DecodeRequest& rq) {
-  if (rq.persistent) {
-    decode_persistent(rq);
+void Decoder::decode(const DecodeRequest& rq_in) {
+  const DecodeRequest rq = rq_in.auto_schedule ? resolve(rq_in) : rq_in;
+  if (rq.graph && rq.device_memory && rq.n_cb > 0) {
+    decode_graph(rq);
     return;
   }
   std::lock_guard<std::mutex> lock(mu_);
+  if (rq.persistent)
+    decode_persistent(rq);
+  else
+    decode_plain(rq);
+}
+
+// ------------------------------------------------------------------------------------------
+// Autotuner
+// ------------------------------------------------------------------------------------------
+std::string Decoder::signature(const DecodeRequest& rq) {
+  double sum_k = 0.0;
+  for (size_t i = 0; i < rq.n_cb; ++i) sum_k += rq.cbs[i].k;
+  const int mean_k = rq.n_cb ? static_cast<int>(std::lround(sum_k / rq.n_cb / 512.0)) * 512 : 0;
+  const int n_log2 = rq.n_cb ? static_cast<int>(std::lround(std::log2(static_cast<double>(rq.n_cb)))) : 0;
+  std::ostringstream o;
+  o << "es=" << (rq.early_stop ? 1 : 0) << ",it=" << rq.max_iterations << ",n~2^" << n_log2
+    << ",meanK~" << mean_k << ",guard=" << rq.guard;
+  return o.str();
+}
+
+DecodeRequest Decoder::resolve(const DecodeRequest& rq) {
+  DecodeRequest r = rq;
+  r.auto_schedule = false;
+  const std::string sig = signature(rq);
+  std::lock_guard<std::mutex> lock(mu_);
+  for (const auto& kv : tuning_)
+    if (kv.first == sig) {
+      r.persistent = kv.second.persistent;
+      if (rq.window == 0) r.window = kv.second.window;
+      return r;
+    }
+  return r;  // untuned: plain schedule, default window
+}
+
+Decoder::TuneChoice Decoder::autotune(const DecodeRequest& rq_in) {
+  if (!rq_in.device_memory) throw InvalidArgument("autotuning needs device-memory buffers");
+  if (rq_in.n_cb == 0) throw InvalidArgument("nothing to tune");
+  struct Cand {
+    bool persistent;
+    int window;
+  };
+  const Cand cands[] = {{false, 128}, {false, 144}, {false, 160}, {false, 168}, {false, 176},
+                        {false, 192}, {false, 224}, {false, 256}, {true, 192}, {true, 256},
+                        {true, 320}};
+  cudaStream_t st = static_cast<cudaStream_t>(rq_in.stream);
+  cudaEvent_t a, b;
+  check(cudaEventCreate(&a), "cudaEventCreate");
+  check(cudaEventCreate(&b), "cudaEventCreate");
+  TuneChoice best;
+  best.ms = 1e30;
+  const int guard = rq_in.guard < 0 ? kDefaultGuard : rq_in.guard;
+  try {
+    for (const Cand& c : cands) {
+      if (c.window < guard) continue;
+      DecodeRequest r = rq_in;
+      r.auto_schedule = false;
+      r.graph = false;
+      r.persistent = c.persistent;
+      r.window = c.window;
+      decode(r);  // warm-up (sizes the workspace)
+      check(cudaEventRecord(a, st), "cudaEventRecord");
+      decode(r);
+      decode(r);
+      check(cudaEventRecord(b, st), "cudaEventRecord");
+      check(cudaEventSynchronize(b), "cudaEventSynchronize");
+      float ms = 0.0f;
+      check(cudaEventElapsedTime(&ms, a, b), "cudaEventElapsedTime");
+      if (ms / 2 < best.ms) best = TuneChoice{c.persistent, c.window, ms / 2.0};
+    }
+  } catch (...) {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    throw;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  const std::string sig = signature(rq_in);
+  std::lock_guard<std::mutex> lock(mu_);
+  for (auto& kv : tuning_)
+    if (kv.first == sig) {
+      kv.second = best;
+      return best;
+    }
+  tuning_.emplace_back(sig, best);
+  return best;
+}
+
+void Decoder::save_tuning(const std::string& path) {
+  std::lock_guard<std::mutex> lock(mu_);
+  std::ofstream f(path);
+  if (!f) throw InvalidArgument("cannot open the tuning file for writing");
+  f << "# turbo_cpp_b200 autotuning table: signature schedule window ms\n";
+  for (const auto& kv : tuning_)
+    f << kv.first << ' ' << (kv.second.persistent ? "persistent" : "plain") << ' '
+      << kv.second.window << ' ' << kv.second.ms << '\n';
+}
+
+void Decoder::load_tuning(const std::string& path) {
+  std::ifstream f(path);
+  if (!f) throw InvalidArgument("cannot open the tuning file");
+  std::vector<std::pair<std::string, TuneChoice>> t;
+  std::string line;
+  while (std::getline(f, line)) {
+    if (line.empty() || line[0] == '#') continue;
+    std::istringstream in(line);
+    std::string sig, sched;
+    TuneChoice c;
+    if (!(in >> sig >> sched >> c.window >> c.ms) || (sched != "plain" && sched != "persistent") ||
+        c.window <= 0 || c.window % kGroup != 0)
+      throw InvalidArgument("malformed tuning file line: " + line);
+    c.persistent = sched == "persistent";
+    t.emplace_back(sig, c);
+  }
+  std::lock_guard<std::mutex> lock(mu_);
+  tuning_ = std::move(t);
+}
+
+// Capture-once / replay: the key covers everything baked into the captured launches (block
+// descriptors, buffer addresses, options, scales); a workspace reallocation invalidates it.
+void Decoder::decode_graph(const DecodeRequest& rq) {
+  std::lock_guard<std::mutex> lock(mu_);
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  cudaStream_t st = static_cast<cudaStream_t>(rq.stream);
+  std::string key;
+  auto put = [&key](const void* p, size_t n) { key.append(static_cast<const char*>(p), n); };
+  const uintptr_t ptrs[4] = {reinterpret_cast<uintptr_t>(rq.llr),
+                             reinterpret_cast<uintptr_t>(rq.posterior),
+                             reinterpret_cast<uintptr_t>(rq.crc_ok),
+                             reinterpret_cast<uintptr_t>(rq.iterations_used)};
+  const int64_t opts[8] = {static_cast<int64_t>(rq.n_cb), static_cast<int64_t>(rq.llr_len),
+                           static_cast<int64_t>(rq.post_len), rq.max_iterations, rq.early_stop,
+                           rq.window, rq.guard, (rq.persistent ? 2 : 0) | (rq.smem_checkpoints ? 1 : 0)};
+  put(ptrs, sizeof ptrs);
+  put(opts, sizeof opts);
+  put(rq.cbs, rq.n_cb * sizeof(CodeBlockDesc));
+  if (rq.scales) put(rq.scales, 2 * rq.max_iterations * sizeof(float));
+  GraphEntry* hit = nullptr;
+  for (auto it = graphs_.begin(); it != graphs_.end(); ++it)
+    if (it->key == key) {
+      if (it->generation == generation_) {
+        graphs_.splice(graphs_.begin(), graphs_, it);  // most recently used first
+        hit = &graphs_.front();
+      } else {
+        drop_graph(*it);
+        graphs_.erase(it);
+      }
+      break;
+    }
+  if (hit == nullptr) {
+    // size the workspace and the descriptor uploads first (outside the capture), so that
+    // capturing allocates nothing
+    upload_bytes_ = 0;
+    {
+      DecodeRequest dry = rq;
+      dry.graph = false;
+      if (rq.persistent) decode_persistent(dry); else decode_plain(dry);
+    }
+    graphs_.emplace_front();
+    GraphEntry& e = graphs_.front();
+    e.key = key;
+    e.arena_bytes = upload_bytes_;
+    check(cudaMallocHost(&e.arena, std::max<size_t>(e.arena_bytes, 256)), "cudaMallocHost");
+    const uint64_t launches_before = timing_.launches;
+    const bool timing_was = timing_on_;
+    timing_on_ = false;
+    capturing_ = &e;
+    cudaGraph_t g = nullptr;
+    check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    try {
+      if (rq.persistent) decode_persistent(rq); else decode_plain(rq);
+    } catch (...) {
+      cudaStreamEndCapture(st, &g);
+      if (g) cudaGraphDestroy(g);
+      capturing_ = nullptr;
+      timing_on_ = timing_was;
+      drop_graph(e);
+      graphs_.pop_front();
+      throw;
+    }
+    check(cudaStreamEndCapture(st, &g), "cudaStreamEndCapture");
+    capturing_ = nullptr;
+    timing_on_ = timing_was;
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    check(ie, "cudaGraphInstantiate");
+    e.exec = exec;
+    e.generation = generation_;
+    e.launches = timing_.launches - launches_before;
+    timing_.launches = launches_before;
+    while (graphs_.size() > 16) {  // keep the most recent 16
+      drop_graph(graphs_.back());
+      graphs_.pop_back();
+    }
+    hit = &e;
+  }
+  order_after_previous(st);
+  check(cudaGraphLaunch(static_cast<cudaGraphExec_t>(hit->exec), st), "cudaGraphLaunch");
+  mark_done(st);
+  timing_.launches += hit->launches;
+}
+
+void Decoder::decode_plain(const DecodeRequest& rq) {
   check(cudaSetDevice(device_), "cudaSetDevice");
   // device memory: the caller's stream as given (NULL = legacy default stream, as in CUDA);
   // host memory: the caller's stream if given, else the decoder's own stream
@@ -306,11 +543,9 @@ void Decoder::decode(const DecodeRequest& rq) {
   float4* ckpt = nullptr;
   if (global_ckpt) ckpt = grow<float4>(d_ckpt_, static_cast<size_t>(n_win) * 2 * max_ckpt);
 
-  check(cudaMemcpyAsync(dcbs, cbs.data(), n * sizeof(DevCb), cudaMemcpyHostToDevice, st), "copy cbs");
-  check(cudaMemcpyAsync(dwin, wincb.data(), n_win * sizeof(int32_t), cudaMemcpyHostToDevice, st),
-        "copy windows");
-  check(cudaMemcpyAsync(dstart, start.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, st),
-        "copy starts");
+  upload(dcbs, cbs.data(), n * sizeof(DevCb), st);
+  upload(dwin, wincb.data(), n_win * sizeof(int32_t), st);
+  upload(dstart, start.data(), n * sizeof(int64_t), st);
   check(cudaMemsetAsync(seeds, 0, static_cast<size_t>(n_win) * 16 * 4 * sizeof(float), st), "zero seeds");
   init_flags_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(
       static_cast<int>(n), done, iters, rq.max_iterations);
@@ -381,7 +616,6 @@ void Decoder::decode(const DecodeRequest& rq) {
 // Persistent schedule: warp tasks of whole code blocks, one launch for all iterations.
 // ------------------------------------------------------------------------------------------
 void Decoder::decode_persistent(const DecodeRequest& rq) {
-  std::lock_guard<std::mutex> lock(mu_);
   check(cudaSetDevice(device_), "cudaSetDevice");
   cudaStream_t st = static_cast<cudaStream_t>(rq.device_memory ? rq.stream
                                                                : (rq.stream ? rq.stream : stream_));
@@ -480,13 +714,10 @@ void Decoder::decode_persistent(const DecodeRequest& rq) {
     post = grow<float>(d_post_, rq.post_len);
     check(cudaMemsetAsync(post, 0, rq.post_len * sizeof(float), st), "zero posterior");
   }
-  check(cudaMemcpyAsync(dcbs, cbs.data(), n * sizeof(DevCb), cudaMemcpyHostToDevice, st), "copy cbs");
-  check(cudaMemcpyAsync(dwin, wincb.data(), n_win * sizeof(int32_t), cudaMemcpyHostToDevice, st),
-        "copy windows");
-  check(cudaMemcpyAsync(dstart, start.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, st),
-        "copy starts");
-  check(cudaMemcpyAsync(dtasks, tasks.data(), tasks.size() * sizeof(int32_t),
-                        cudaMemcpyHostToDevice, st), "copy tasks");
+  upload(dcbs, cbs.data(), n * sizeof(DevCb), st);
+  upload(dwin, wincb.data(), n_win * sizeof(int32_t), st);
+  upload(dstart, start.data(), n * sizeof(int64_t), st);
+  upload(dtasks, tasks.data(), tasks.size() * sizeof(int32_t), st);
   check(cudaMemsetAsync(dqueue, 0, (2 + static_cast<size_t>(n_tasks)) * sizeof(int), st),
         "zero queue");
   check(cudaMemsetAsync(seeds, 0, static_cast<size_t>(n_win) * 16 * 4 * sizeof(float), st),
@@ -505,6 +736,7 @@ void Decoder::decode_persistent(const DecodeRequest& rq) {
   a.n_tasks = n_tasks;
   a.queue = dqueue;
   a.error = static_cast<int*>(d_err_.ptr);
+  a.stall_task = stall_task_;
   a.progress = dqueue + 2;
   a.llr = llr;
   a.sys_i = sysi;

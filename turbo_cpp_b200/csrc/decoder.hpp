@@ -2,6 +2,8 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <list>
+#include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -59,6 +61,8 @@ struct DecodeRequest {
   bool device_memory = false;  // llr/posterior/crc_ok/iterations_used are device pointers
   bool smem_checkpoints = false;  // alpha checkpoints in shared memory instead of global scratch
   bool persistent = false;  // persistent warp-task schedule instead of per-half-iteration launches
+  bool graph = false;       // device memory: capture the launch sequence once, replay it after
+  bool auto_schedule = false;  // take schedule and window from the autotuning table
   const float* scales = nullptr;  // host; 2 per iteration (upper, lower); null = all 1
   void* stream = nullptr;
 };
@@ -90,12 +94,48 @@ class Decoder {
   int device() const { return device_; }
   void set_timing(bool on);
   void sync();  // waits for this decoder's enqueued work; reports a persistent wait timeout
+  void inject_stall(int task) { stall_task_ = task; }  // testing hook (-1: off)
+
+  // Autotuning: times candidate (schedule, window) pairs on a device-memory request and keeps
+  // the fastest for requests with the same signature.
+  struct TuneChoice {
+    bool persistent = false;
+    int window = 0;
+    double ms = 0.0;
+  };
+  TuneChoice autotune(const DecodeRequest& rq);
+  void save_tuning(const std::string& path);
+  void load_tuning(const std::string& path);
+  static std::string signature(const DecodeRequest& rq);
   Timing timing(bool reset);  // waits for the recorded events
   int sm_count() const { return sm_count_; }
 
  private:
   int pick_window(int32_t k, int32_t requested) const;
   void decode_persistent(const DecodeRequest& rq);
+  void decode_plain(const DecodeRequest& rq);
+  void decode_graph(const DecodeRequest& rq);
+  // host -> device copy of launch descriptors; while capturing, from graph-owned pinned memory
+  void upload(void* dst, const void* src, size_t bytes, void* stream);
+  template <class T>
+  T* grow(DeviceBuffer& b, size_t count);
+
+  // CUDA graphs of previously seen device-memory requests (same shapes, pointers, options)
+  struct GraphEntry {
+    std::string key;
+    uint64_t generation = 0;
+    void* exec = nullptr;                 // cudaGraphExec_t
+    void* arena = nullptr;                // pinned host copies of the descriptors
+    size_t arena_bytes = 0, arena_used = 0;
+    uint64_t launches = 0;
+  };
+  std::list<GraphEntry> graphs_;
+  std::vector<std::pair<std::string, TuneChoice>> tuning_;
+  DecodeRequest resolve(const DecodeRequest& rq);  // applies the tuning table to an auto request
+  GraphEntry* capturing_ = nullptr;       // entry being captured (uploads go to its staging)
+  uint64_t generation_ = 0;               // bumped whenever a workspace buffer moves
+  size_t upload_bytes_ = 0;               // descriptor bytes uploaded (sizes a graph's arena)
+  void drop_graph(GraphEntry& e);
   void record_start(void* stream);
   void record_stop(void* stream, uint64_t steps);
 
@@ -120,6 +160,7 @@ class Decoder {
       d_done_, d_iters_, d_crc_, d_ckpt_, d_tasks_, d_queue_;
   int persist_blocks_per_sm_ = 0;
   DeviceBuffer d_err_;          // sticky: set by a persistent-schedule wait that gave up
+  int stall_task_ = -1;
   void* last_event_ = nullptr;  // completion of the previous decode (orders workspace reuse)
   void order_after_previous(void* stream);
   void mark_done(void* stream);
