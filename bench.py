@@ -55,7 +55,8 @@ def parse():
     ap.add_argument("--iterations", type=int, default=8)
     ap.add_argument("--window", type=int, default=0)
     ap.add_argument("--guard", type=int, default=-1)
-    ap.add_argument("--schedule", choices=["plain", "persistent"], default="plain")
+    ap.add_argument("--schedule", choices=["auto", "plain", "persistent"], default="auto")
+    ap.add_argument("--no-graph", action="store_true", help="launch without CUDA graph replay")
     ap.add_argument("--points", type=int, default=len(EBN0), help="Eb/N0 points to use")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -240,8 +241,7 @@ def workload_config(args):
                     f"{args.n_cb} code blocks per call, exact Log-MAP, {args.iterations} "
                     "iterations, no early stop, Eb/N0 0.0..1.2 dB step 0.2",
         "n_cb": args.n_cb, "k": K, "iterations": args.iterations,
-        "window": args.window or 128, "guard": 96 if args.guard < 0 else args.guard,
-        "schedule": args.schedule, "ebn0_db": EBN0[:args.points],
+        "guard": 96 if args.guard < 0 else args.guard, "ebn0_db": EBN0[:args.points],
         "l2": "inputs 302 MB per step > 126 MB L2 (no flush needed)",
     }
 
@@ -265,9 +265,6 @@ def main():
     torch.cuda.set_device(local)
     dev = tc.Decoder(local)
     n, it = args.n_cb, args.iterations
-    opts = tc.DecodeOptions(it, False, args.window, args.guard,
-                            tc.SCHEDULE_PERSISTENT if args.schedule == "persistent"
-                            else tc.SCHEDULE_PLAIN)
     cbs, llr_len, post_len = tc.Decoder.layout([K] * n)
     points = EBN0[:args.points]
     batches, truth = [], []
@@ -280,10 +277,24 @@ def main():
     stream.wait_stream(torch.cuda.current_stream())
     torch.cuda.set_stream(stream)
 
-    def step(i):
+    # ---- schedule and window: autotuned on this workload unless given ----
+    if args.schedule == "auto" and args.window == 0:
+        tuned = dev.autotune(cbs, n, batches[0].data_ptr(), llr_len, post.data_ptr(), post_len,
+                             tc.DecodeOptions(it, False, 0, args.guard), stream.cuda_stream)
+        sched = tc.SCHEDULE_AUTO
+    else:
+        tuned = None
+        sched = {"plain": tc.SCHEDULE_PLAIN, "persistent": tc.SCHEDULE_PERSISTENT,
+                 "auto": tc.SCHEDULE_AUTO}[args.schedule]
+    opts = tc.DecodeOptions(it, False, args.window, args.guard, sched, graph=not args.no_graph)
+    schedule_name = (("persistent" if tuned["schedule"] == 1 else "plain") if tuned
+                     else args.schedule)
+    window = tuned["window"] if tuned else (args.window or 128)
+
+    def step(i, o=opts):
         x = batches[i % len(batches)]
         dev.decode_device(cbs, n, x.data_ptr(), llr_len, post.data_ptr(), post_len,
-                          options=opts, stream=stream.cuda_stream)
+                          options=o, stream=stream.cuda_stream)
 
     # BER/BLER per point (outside the timed region)
     quality = []
@@ -293,11 +304,11 @@ def main():
         ber, bler = ber_bler(post.cpu().numpy(), truth[j], n, K)
         quality.append({"ebn0_db": points[j], "ber": ber, "bler": bler, "blocks": n})
 
+    # ---- timed region: the batched decoder as a user runs it ----
     for i in range(args.warmup):
         step(i)
     stream.synchronize()
-    dev.timing(reset=True)
-    dev.set_timing(True)
+    tm0 = dev.timing(reset=True)
     barrier(world)
     torch.cuda.synchronize()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -308,12 +319,38 @@ def main():
         t1.record(stream)
         torch.cuda.synchronize()
     barrier(world)
-    dev.set_timing(False)
-    tm = dev.timing(reset=True)
+    launches = dev.timing(reset=True)["launches"]
     ms = max_over_ranks(t0.elapsed_time(t1), world)
     bits_total = world * n * K * args.steps
     value = bits_total / (ms / 1e3) / 1e6
     clocks = clk.summary()
+
+    # ---- dominant kernel: CUDA events around each of its launches, same schedule ----
+    kern_opts = tc.DecodeOptions(it, False, window, args.guard,
+                                 tc.SCHEDULE_PERSISTENT if schedule_name == "persistent"
+                                 else tc.SCHEDULE_PLAIN)
+    dev.set_timing(True)
+    for i in range(3):
+        step(i, kern_opts)
+    stream.synchronize()
+    dev.set_timing(False)
+    tm = dev.timing(reset=True)
+
+    # ---- the two schedules at fixed windows, for the record ----
+    def mbps_of(o, reps=3):
+        step(0, o)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(reps):
+            step(i, o)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return n * K * reps / (e0.elapsed_time(e1) / 1e3) / 1e6
+    schedules = {
+        "plain_w128": mbps_of(tc.DecodeOptions(it, False, 128, args.guard, tc.SCHEDULE_PLAIN)),
+        "persistent_w192": mbps_of(tc.DecodeOptions(it, False, 192, args.guard,
+                                                    tc.SCHEDULE_PERSISTENT)),
+    }
 
     # ---- end to end through the C ABI with pinned host buffers ----
     e2e = None
@@ -326,7 +363,8 @@ def main():
         host_it = torch.empty(n, dtype=torch.int32).pin_memory()
         import ctypes
 
-        host_opt, _keep = dev._opts(opts, tc.MEM_HOST)
+        host_opt, _keep = dev._opts(tc.DecodeOptions(it, False, window, args.guard,
+                                                     kern_opts.schedule), tc.MEM_HOST)
 
         def host_step(i):
             x = host_llr[i % len(host_llr)]
@@ -337,38 +375,45 @@ def main():
             host_step(i)
         barrier(world)
         t = time.perf_counter()
-        for i in range(args.steps):
+        e2e_steps = max(3, args.steps // 2)
+        for i in range(e2e_steps):
             host_step(i)
         e2e_s = max_over_ranks(time.perf_counter() - t, world)
-        e2e = {"value": bits_total / e2e_s / 1e6, "unit": "Mbit/s",
+        e2e = {"value": world * n * K * e2e_steps / e2e_s / 1e6, "unit": "Mbit/s",
                "h2d_bytes_per_step": llr_len * 4, "d2h_bytes_per_step": post_len * 4 + n * 5,
-               "timing": "wall clock around synchronous tc_decode calls, max over ranks"}
+               "timing": "wall clock around synchronous tc_decode calls (TC_MEM_HOST, pinned "
+                         "buffers), max over ranks"}
 
-    # ---- roofline of the dominant kernel (SISO launch), from the live CUDA-event timings ----
+    # ---- roofline of the dominant kernel, from the live CUDA-event timings ----
     props = torch.cuda.get_device_properties(local)
     sm_mhz = clocks["sm_mhz"] or 1965.0
     avg_launch_ms = tm["siso_ms"] / max(tm["siso_launches"], 1)
     steps_per_launch = tm["trellis_steps"] / max(tm["siso_launches"], 1)
     achieved = TRANSC_PER_STEP * steps_per_launch / (avg_launch_ms / 1e3) / 1e9
     peak = props.multi_processor_count * MUFU_PER_SM_CLK * sm_mhz * 1e6 / 1e9
-    traffic_per_step = ncu_traffic(args.schedule)
+    traffic_per_step = ncu_traffic(schedule_name)
     hbm_peak, hbm_src = measured_peaks()
-    alg_bytes_launch = steps_per_launch * BYTES_PER_BIT / 2 / it  # share of one decode's bytes
+    # algorithmic bytes of the launch: its share of the decode's 16 B per info bit
+    alg_bytes_launch = steps_per_launch * BYTES_PER_BIT / (2 * it)
     hbm_achieved = alg_bytes_launch / (avg_launch_ms / 1e3) / 1e9
+    kernel_name = ("persistent_kernel (all iterations of all code blocks, device work queue)"
+                   if schedule_name == "persistent"
+                   else "siso_plain_kernel (one SISO half-iteration over all code blocks)")
     line = {
         "metric": METRIC, "value": value, "unit": "Mbit/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: seeded uniform info bits, BPSK/AWGN at Eb/N0 0.0..1.2 dB (one batch "
                 "per point, steps cycle through them), FP32 LLRs 2y/sigma^2",
-        "config": workload_config(args),
+        "config": dict(workload_config(args), schedule=schedule_name, window=window,
+                       autotuned=tuned is not None, cuda_graph=not args.no_graph),
         "roofline": {
             "bound": "sfu", "achieved": achieved, "peak": peak, "unit": "Gtransc/s",
             "frac": achieved / peak, "traffic": None if traffic_per_step is None
             else traffic_per_step * steps_per_launch,
-            "kernel": "siso_plain_kernel (one SISO half-iteration over all code blocks)",
-            "work": f"{TRANSC_PER_STEP} transcendentals per trellis step (30 exact max*), "
-                    f"{steps_per_launch:.0f} steps per launch",
+            "kernel": kernel_name,
+            "work": f"{TRANSC_PER_STEP} transcendentals per trellis step per SISO (30 exact "
+                    f"max*), {steps_per_launch:.0f} SISO steps per launch",
             "avg_launch_ms": avg_launch_ms,
             "peak_source": f"{props.multi_processor_count} SMs x {MUFU_PER_SM_CLK} MUFU/clk x "
                            f"median sampled SM clock {sm_mhz:.0f} MHz (nominal issue rate)",
@@ -376,13 +421,16 @@ def main():
         "roofline_hbm": {
             "bound": "hbm", "achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
             "frac": hbm_achieved / hbm_peak, "peak_source": f"{hbm_src} MEASURED_PEAKS hbm_gbs",
-            "work": "16.0 B per info bit per decode (3(K+4) LLRs in, K posteriors out), split "
-                    "over the 2*iterations SISO launches",
+            "work": "16.0 B per info bit per decode (3(K+4) LLRs in, K posteriors out), the "
+                    "launch's share",
         },
-        "gpu_launches": int(tm["launches"]),
+        "gpu_launches": int(launches),
         "clocks": clocks,
+        "schedules_mbps": schedules,
         "ber_bler": quality,
     }
+    if tuned:
+        line["autotune"] = tuned
     if e2e:
         line["e2e"] = e2e
     # ---- plain per-block GPU path: one code block per call, as the reference API decodes ----
@@ -391,7 +439,8 @@ def main():
     for r in range(2):
         t = time.perf_counter()
         for c in range(8):
-            dev.decode([K], sub[c * 3 * (K + 4):(c + 1) * 3 * (K + 4)], options=opts)
+            dev.decode([K], sub[c * 3 * (K + 4):(c + 1) * 3 * (K + 4)],
+                       options=tc.DecodeOptions(it))
         if r:
             per_block.append(8 * K / (time.perf_counter() - t) / 1e6)
     line["plain_per_block"] = {"value": float(np.mean(per_block)), "unit": "Mbit/s",
