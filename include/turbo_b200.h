@@ -166,6 +166,43 @@ TC_API int tc_decode(tc_decoder* dec, size_t n_cb, const tc_code_block* cbs, siz
               const float* llr, size_t post_len, float* posterior, uint8_t* crc_ok,
               uint32_t* iterations_used, const tc_decode_options* opts);
 
+/* ---------------- transport-block chain on the device (new) ----------------
+ * LLR-domain de-rate matching of many code blocks on the GPU: bit-identical to
+ * tc_derate_match_llr (the reference's walk of lte_turbo.cpp:280-325 with soft values).  e_llr
+ * and d012 are device pointers; ordered on `stream` (NULL = legacy default stream). */
+typedef struct {
+  int32_t k;          /* block size                                                  */
+  int32_t filler;     /* filler bits (first code block of a transport block)         */
+  int32_t e;          /* rate-matched LLRs of the block                               */
+  uint32_t rv;        /* redundancy version 0..3                                      */
+  int64_t e_offset;   /* float offset of its E rate-matched LLRs                     */
+  int64_t llr_offset; /* float offset of its [d0|d1|d2] output (multiple of 4)       */
+} tc_rm_block;
+TC_API int tc_derate_match_llr_device(tc_decoder* dec, size_t n_cb, const tc_rm_block* blocks,
+                                      size_t e_len, const float* e_llr, size_t llr_len,
+                                      float* d012, void* stream);
+
+/* Decodes many transport blocks at once (replaces decode_transport_block, lte_turbo.h:157-159,
+ * lte_turbo.cpp:891-980, for any number of transport blocks per call): device de-rate matching,
+ * batched turbo decoding with opts (schedule, early stop on CRC24B, iterations, ...), then per
+ * transport block hard decisions, filler strip, CRC24B check and strip (C > 1), concatenation
+ * and CRC24A.  The code blocks of transport block t are cbs[first_cb .. first_cb + n_cb); their
+ * llr_offset is ignored.  tb_bits receives one byte (0/1) per decoded bit at bits_offset;
+ * tb_crc_ok (n_tb), cb_crc_ok, iterations_used (n_cb) and posterior (sum K, may be NULL) follow
+ * opts->memory like the rate-matched LLRs. */
+typedef struct {
+  int64_t tbs;         /* transport block size, without CRC24A */
+  int32_t first_cb;
+  int32_t n_cb;
+  int64_t bits_offset; /* first output bit of the block */
+} tc_transport_block;
+TC_API int tc_decode_transport_blocks(tc_decoder* dec, size_t n_tb, const tc_transport_block* tbs,
+                                      size_t n_cb, const tc_rm_block* cbs, size_t e_len,
+                                      const float* e_llr, size_t bits_len, uint8_t* tb_bits,
+                                      uint8_t* tb_crc_ok, uint8_t* cb_crc_ok,
+                                      uint32_t* iterations_used, float* posterior,
+                                      const tc_decode_options* opts);
+
 /* ---------------- decoding without device allocation ----------------
  * No counterpart in the reference.  The same plain-schedule decode as tc_decode with
  * TC_MEM_DEVICE, for callers that must not allocate device memory: a real-time receiver thread

@@ -82,6 +82,16 @@ class _Options(C.Structure):
                 ("scales", C.c_void_p), ("graph", C.c_uint32), ("stream", C.c_void_p)]
 
 
+class _RmBlock(C.Structure):
+    _fields_ = [("k", C.c_int32), ("filler", C.c_int32), ("e", C.c_int32), ("rv", C.c_uint32),
+                ("e_offset", C.c_int64), ("llr_offset", C.c_int64)]
+
+
+class _TransportBlock(C.Structure):
+    _fields_ = [("tbs", C.c_int64), ("first_cb", C.c_int32), ("n_cb", C.c_int32),
+                ("bits_offset", C.c_int64)]
+
+
 class _TuneResult(C.Structure):
     _fields_ = [("schedule", C.c_int32), ("window", C.c_int32), ("ms", C.c_double)]
 
@@ -119,6 +129,9 @@ _SIGNATURES = {
     "tc_decode": [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, _VP, _VP, _VP],
     "tc_decode_noalloc": [_SZ, _VP, _SZ, _VP, _SZ, _VP, _VP, _VP, _VP, _VP],
     "tc_decoder_sync": [_VP],
+    "tc_derate_match_llr_device": [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, _VP],
+    "tc_decode_transport_blocks": [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, _VP, _VP, _VP,
+                                   _VP, _VP],
     "tc_decoder_inject_stall": [_VP, C.c_int],
     "tc_autotune": [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, _VP, _VP],
     "tc_autotune_save": [_VP, C.c_char_p],
@@ -513,6 +526,60 @@ class Decoder:
         _call("tc_autotune", self._h, int(n_cb), C.addressof(cbs), int(llr_len), llr_ptr,
               int(post_len), post_ptr, C.addressof(opt), C.addressof(r))
         return {"schedule": r.schedule, "window": r.window, "ms": r.ms}
+
+    @staticmethod
+    def rm_blocks(blocks):
+        """tc_rm_block array from (k, filler, e, rv) tuples; E LLRs back to back, outputs
+        [d0|d1|d2] back to back."""
+        arr = (_RmBlock * max(len(blocks), 1))()
+        e_off = llr_off = 0
+        for i, (k, f, e, rv) in enumerate(blocks):
+            arr[i].k, arr[i].filler, arr[i].e, arr[i].rv = int(k), int(f), int(e), int(rv)
+            arr[i].e_offset, arr[i].llr_offset = e_off, llr_off
+            e_off += int(e)
+            llr_off += 3 * (int(k) + 4)
+        return arr, e_off, llr_off
+
+    def derate_device(self, blocks, e_ptr: int, e_len: int, out_ptr: int, llr_len: int,
+                      stream: int = 0) -> None:
+        """LLR-domain de-rate matching on the GPU (device pointers)."""
+        arr, _, _ = self.rm_blocks(blocks)
+        _call("tc_derate_match_llr_device", self._h, len(blocks), C.addressof(arr), int(e_len),
+              e_ptr, int(llr_len), out_ptr, stream or None)
+
+    def decode_tbs(self, tbs, blocks, e_llr, options: Optional[DecodeOptions] = None,
+                   want_posterior: bool = False):
+        """Many transport blocks through the device chain (host arrays): tbs = list of
+        (TBS, n_cb); blocks = (k, filler, e, rv) per code block in transport-block order;
+        e_llr = their rate-matched LLRs back to back.  Returns (bits per TB, tb_crc_ok,
+        cb_crc_ok, iterations per code block[, posterior])."""
+        o = options or DecodeOptions()
+        arr, e_len, _ = self.rm_blocks(blocks)
+        x = np.ascontiguousarray(e_llr, np.float32)
+        if x.size != e_len:
+            raise InvalidArgument(f"expected {e_len} rate-matched LLRs, got {x.size}")
+        tba = (_TransportBlock * max(len(tbs), 1))()
+        first = bits = 0
+        for i, (size, ncb) in enumerate(tbs):
+            tba[i].tbs, tba[i].first_cb, tba[i].n_cb, tba[i].bits_offset = (
+                int(size), first, int(ncb), bits)
+            first += int(ncb)
+            bits += int(size)
+        out = np.zeros(bits, np.uint8)
+        tb_ok = np.zeros(len(tbs), np.uint8)
+        cb_ok = np.zeros(len(blocks), np.uint8)
+        it = np.zeros(len(blocks), np.uint32)
+        post = np.zeros(sum(int(b[0]) for b in blocks), np.float32) if want_posterior else None
+        opt, _keep = self._opts(o, MEM_HOST)
+        _call("tc_decode_transport_blocks", self._h, len(tbs), C.addressof(tba), len(blocks),
+              C.addressof(arr), e_len, _ptr(x), bits, _ptr(out), _ptr(tb_ok), _ptr(cb_ok),
+              _ptr(it), _ptr(post) if post is not None else None, C.addressof(opt))
+        per_tb, pos = [], 0
+        for size, _ in tbs:
+            per_tb.append(out[pos:pos + int(size)])
+            pos += int(size)
+        res = (per_tb, tb_ok.astype(bool), cb_ok.astype(bool), it)
+        return res + (post,) if want_posterior else res
 
     def save_tuning(self, path: str) -> None:
         _call("tc_autotune_save", self._h, os.fsencode(path))

@@ -373,6 +373,55 @@ int tc_decoder_sync(tc_decoder* dec) {
   });
 }
 
+int tc_derate_match_llr_device(tc_decoder* dec, size_t n_cb, const tc_rm_block* blocks,
+                               size_t e_len, const float* e_llr, size_t llr_len, float* d012,
+                               void* stream) {
+  return guarded([&] {
+    need(dec != nullptr && (n_cb == 0 || (blocks && e_llr && d012)), "null pointer");
+    static_assert(sizeof(tc_rm_block) == sizeof(tcb::RmBlockDesc), "descriptor layout");
+    dec->impl.derate_match_llr(n_cb, reinterpret_cast<const tcb::RmBlockDesc*>(blocks), e_llr,
+                               e_len, d012, llr_len, stream);
+  });
+}
+
+int tc_decode_transport_blocks(tc_decoder* dec, size_t n_tb, const tc_transport_block* tbs,
+                               size_t n_cb, const tc_rm_block* cbs, size_t e_len,
+                               const float* e_llr, size_t bits_len, uint8_t* tb_bits,
+                               uint8_t* tb_crc_ok, uint8_t* cb_crc_ok, uint32_t* iterations_used,
+                               float* posterior, const tc_decode_options* opts) {
+  return guarded([&] {
+    need(dec != nullptr, "null decoder");
+    need(n_tb == 0 || (tbs && cbs && e_llr && tb_bits), "null pointer");
+    static_assert(sizeof(tc_transport_block) == sizeof(tcb::TbDesc), "descriptor layout");
+    tc_decode_options o;
+    if (opts) o = *opts; else tc_decode_options_init(&o);
+    need(o.max_iterations <= 64, "max_iterations above 64");
+    need(o.schedule <= TC_SCHEDULE_AUTO, "unknown schedule");
+    tcb::TbRequest q;
+    q.n_tb = n_tb;
+    q.tbs = reinterpret_cast<const tcb::TbDesc*>(tbs);
+    q.n_cb = n_cb;
+    q.cbs = reinterpret_cast<const tcb::RmBlockDesc*>(cbs);
+    q.e_len = e_len;
+    q.e_llr = e_llr;
+    q.bits_len = bits_len;
+    q.bits = tb_bits;
+    q.tb_crc_ok = tb_crc_ok;
+    q.cb_crc_ok = cb_crc_ok;
+    q.iterations_used = iterations_used;
+    q.posterior = posterior;
+    q.device_memory = o.memory == TC_MEM_DEVICE;
+    q.stream = o.stream;
+    q.decode.max_iterations = o.max_iterations;
+    q.decode.early_stop = o.early_stop != 0;
+    q.decode.window = o.window;
+    q.decode.guard = o.guard;
+    q.decode.persistent = o.schedule == TC_SCHEDULE_PERSISTENT;
+    q.decode.scales = o.scales;
+    dec->impl.decode_transport_blocks(q);
+  });
+}
+
 int tc_decoder_set_timing(tc_decoder* dec, int enable) {
   return guarded([&] {
     need(dec != nullptr, "null decoder");

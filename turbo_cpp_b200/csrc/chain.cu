@@ -1,0 +1,311 @@
+// chain.cu -- the decode side of the transport-block chain on the device: LLR-domain de-rate
+// matching, batched turbo decoding (decoder.cu), hard decisions, filler and CRC24B strip,
+// transport-block reassembly and CRC24A.  Batched over many transport blocks per call; the
+// reference does the same per transport block on the host (decode_transport_block,
+// lte_turbo.cpp:891-980, de-rate matching lte_turbo.cpp:280-325).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "decoder.hpp"
+#include "lte_codec.hpp"
+#include "siso.cuh"
+
+namespace tcb {
+namespace {
+
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+__constant__ uint8_t c_col_perm[32] = {0, 16, 8, 24, 4, 20, 12, 28, 2, 18, 10, 26, 6, 22, 14, 30,
+                                       1, 17, 9, 25, 5, 21, 13, 29, 3, 19, 11, 27, 7, 23, 15, 31};
+
+struct DevRm {
+  int32_t k, filler, e, rv;
+  int64_t e_off;  // first rate-matched LLR of the block
+  int64_t out;    // float offset of [d0|d1|d2] (3(K+4) floats)
+};
+
+// Circular-buffer position -> index into [d0|d1|d2], -1 for <NULL> (sub-block interleavers of
+// lte_turbo.cpp:195-236 in closed form; interlacing lte_turbo.cpp:256-262).
+__device__ __forceinline__ int rm_source(int pos, int d, int rows, int kpi, int filler) {
+  const int dummy = kpi - d;
+  if (pos < kpi) {  // systematic, read column by column
+    const int y = (pos % rows) * 32 + c_col_perm[pos / rows] - dummy;
+    return (y < 0 || y < filler) ? -1 : y;
+  }
+  const int local = pos - kpi, lane = local >> 1;
+  if ((local & 1) == 0) {  // parity 1: same permutation as the systematic stream
+    const int y = (lane % rows) * 32 + c_col_perm[lane / rows] - dummy;
+    return (y < 0 || y < filler) ? -1 : d + y;
+  }
+  const int y = (c_col_perm[lane / rows] + 32 * (lane % rows) + 1) % kpi - dummy;
+  return y < 0 ? -1 : 2 * d + y;  // parity 2: no filler nulling
+}
+
+constexpr int kRmThreads = 512;
+
+// One CTA per code block.  The rate-matched LLR k lands on the k-th non-<NULL> position of the
+// circular walk that starts at k0; a valid position of rank r (valid positions before it) is
+// visited by k = (r - rank(k0)) mod Nv, then every Nv further LLRs.  Each stream element gathers
+// its visits in increasing k from 0.0f, which is the reference's summation order, so the result
+// is bit-identical to derate_match_streams with LLR values.
+__global__ void __launch_bounds__(kRmThreads) derate_llr_kernel(const DevRm* __restrict__ blocks,
+                                                                const float* __restrict__ e_llr,
+                                                                float* __restrict__ d012) {
+  __shared__ int warp_sum[kRmThreads / 32];
+  __shared__ int s_rank_k0, s_total;
+  const DevRm b = blocks[blockIdx.x];
+  const int d = b.k + 4, rows = (d + 31) / 32, kpi = rows * 32, ncb = 3 * kpi;
+  const int k0 = rows * (2 * ((ncb + 8 * rows - 1) / (8 * rows)) * b.rv + 2) % ncb;
+  float* out = d012 + b.out;
+  for (int i = threadIdx.x; i < 3 * d; i += blockDim.x) out[i] = 0.0f;
+  // contiguous chunk of positions per thread; count the valid ones
+  const int chunk = (ncb + blockDim.x - 1) / blockDim.x;
+  const int p0 = min(ncb, static_cast<int>(threadIdx.x) * chunk), p1 = min(ncb, p0 + chunk);
+  int cnt = 0;
+  for (int p = p0; p < p1; ++p) cnt += rm_source(p, d, rows, kpi, b.filler) >= 0;
+  // block-wide exclusive scan of the counts
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) warp_sum[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    int v = lane < kRmThreads / 32 ? warp_sum[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += u;
+    }
+    if (lane < kRmThreads / 32) warp_sum[lane] = v;  // inclusive per warp
+  }
+  __syncthreads();
+  const int before = (wid ? warp_sum[wid - 1] : 0) + incl - cnt;
+  if (threadIdx.x == blockDim.x - 1) s_total = before + cnt;
+  if (k0 >= p0 && k0 < p1) {
+    int r = before;
+    for (int p = p0; p < k0; ++p) r += rm_source(p, d, rows, kpi, b.filler) >= 0;
+    s_rank_k0 = r;
+  }
+  __syncthreads();  // also orders the zero fill before the scattered writes
+  const int nv = s_total, r0 = s_rank_k0;
+  const float* x = e_llr + b.e_off;
+  int rank = before;
+  for (int p = p0; p < p1; ++p) {
+    const int src = rm_source(p, d, rows, kpi, b.filler);
+    if (src < 0) continue;
+    int kk = rank - r0;
+    if (kk < 0) kk += nv;
+    float sum = 0.0f;
+    for (; kk < b.e; kk += nv) sum += x[kk];
+    out[src] = sum;
+    ++rank;
+  }
+}
+
+struct DevTb {
+  int32_t first_cb, n_cb;
+  int64_t tbs;       // transport block size without CRC24A
+  int64_t bits_out;  // offset of the block's TBS output bits
+};
+
+// One warp per transport block (lte_turbo.cpp:958-979): hard decisions (>= 0 -> 1), the first
+// code block's filler dropped, CRC24B checked and stripped when C > 1, blocks concatenated, and
+// CRC24A checked over TBS + 24 bits.  A CRC is a syndrome: the XOR of x^(N-1-j) mod g over the
+// set bits j of the N-bit codeword.
+__global__ void tb_finish_kernel(const DevTb* __restrict__ tbs, int n_tb, const DevCb* __restrict__ cbs,
+                                 const float* __restrict__ post, const uint32_t* __restrict__ xpow_a,
+                                 const uint32_t* __restrict__ xpow_b, uint8_t* __restrict__ bits,
+                                 uint8_t* __restrict__ tb_ok, uint8_t* __restrict__ cb_ok) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n_tb) return;
+  const DevTb t = tbs[warp];
+  const int64_t n_a = t.tbs + 24;  // TB codeword length with CRC24A
+  uint32_t syn_a = 0;
+  int64_t pos = 0;  // bit position in the TB + CRC24A stream
+  for (int r = 0; r < t.n_cb; ++r) {
+    const DevCb cb = cbs[t.first_cb + r];
+    const int n_b = cb.k - cb.filler;                        // CRC24B codeword length
+    const int keep = n_b - (t.n_cb > 1 ? 24 : 0);            // bits that join the TB stream
+    uint32_t syn_b = 0;
+    for (int i = lane; i < n_b; i += 32) {
+      const uint8_t bit = post[cb.out + cb.filler + i] >= 0.0f ? 1 : 0;
+      if (bit) syn_b ^= xpow_b[n_b - 1 - i];
+      if (i < keep) {
+        const int64_t j = pos + i;
+        if (bit && j < n_a) syn_a ^= xpow_a[n_a - 1 - j];
+        if (j < t.tbs) bits[t.bits_out + j] = bit;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) syn_b ^= __shfl_xor_sync(0xffffffffu, syn_b, o);
+    if (lane == 0) cb_ok[t.first_cb + r] = (t.n_cb == 1) ? 1 : (syn_b == 0);
+    pos += keep;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) syn_a ^= __shfl_xor_sync(0xffffffffu, syn_a, o);
+  if (lane == 0) tb_ok[warp] = (pos == n_a) && syn_a == 0;
+}
+
+std::vector<uint32_t> xpow_table(CrcKind kind, size_t n) {
+  std::vector<uint32_t> t(n);
+  const uint32_t g = crc_generator_mask(kind);
+  uint32_t r = 1;
+  for (size_t j = 0; j < n; ++j) {
+    t[j] = r;
+    r <<= 1;
+    if (r & (1u << 24)) r ^= (1u << 24) | g;
+  }
+  return t;
+}
+
+}  // namespace
+
+// d012 = de-rate-matched LLRs of every block ([d0|d1|d2] each, at blocks[i].llr_offset).
+void Decoder::derate_device(size_t n, const RmBlockDesc* blocks, const float* e_llr, size_t e_len,
+                            float* d012, size_t llr_len, void* stream) {
+  std::vector<DevRm> v(n);
+  for (size_t i = 0; i < n; ++i) {
+    const RmBlockDesc& b = blocks[i];
+    if (qpp_index(b.k) < 0) throw OutOfRange("unsupported QPP block size");
+    if (b.filler < 0 || b.filler >= b.k || b.rv > 3 || b.e < 0)
+      throw InvalidArgument("invalid filler count, rv or E");
+    if (b.e_offset < 0 || static_cast<size_t>(b.e_offset) + static_cast<size_t>(b.e) > e_len)
+      throw InvalidArgument("rate-matched LLRs out of range");
+    if (b.llr_offset < 0 || b.llr_offset % 4 != 0 ||
+        static_cast<size_t>(b.llr_offset) + 3 * static_cast<size_t>(b.k + 4) > llr_len)
+      throw InvalidArgument("invalid LLR offset (must be a multiple of 4 and in range)");
+    v[i] = DevRm{b.k, b.filler, b.e, static_cast<int32_t>(b.rv), b.e_offset, b.llr_offset};
+  }
+  if (n == 0) return;
+  DevRm* d = grow<DevRm>(d_rm_, n);
+  upload(d, v.data(), n * sizeof(DevRm), stream);
+  derate_llr_kernel<<<static_cast<unsigned>(n), kRmThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      d, e_llr, d012);
+  check(cudaGetLastError(), "de-rate launch");
+  timing_.launches += 1;
+}
+
+void Decoder::derate_match_llr(size_t n, const RmBlockDesc* blocks, const float* e_llr,
+                               size_t e_len, float* d012, size_t llr_len, void* stream) {
+  std::lock_guard<std::mutex> lock(mu_);
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  order_after_previous(stream);
+  derate_device(n, blocks, e_llr, e_len, d012, llr_len, stream);
+  mark_done(stream);
+}
+
+void Decoder::decode_transport_blocks(const TbRequest& q) {
+  std::lock_guard<std::mutex> lock(mu_);
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  cudaStream_t st = static_cast<cudaStream_t>(q.device_memory ? q.stream
+                                                              : (q.stream ? q.stream : stream_));
+  order_after_previous(st);
+  // ---- validate the transport blocks and lay out their code blocks ----
+  std::vector<DevTb> tbs(q.n_tb);
+  std::vector<RmBlockDesc> rm(q.n_cb);
+  std::vector<CodeBlockDesc> cbs(q.n_cb);
+  int64_t llr_len = 0, post_len = 0, bits_len = 0;
+  for (size_t i = 0; i < q.n_cb; ++i) {
+    rm[i] = q.cbs[i];
+    rm[i].llr_offset = llr_len;
+    cbs[i] = CodeBlockDesc{q.cbs[i].k, q.cbs[i].filler, llr_len, post_len};
+    llr_len += 3 * static_cast<int64_t>(q.cbs[i].k + 4);
+    post_len += q.cbs[i].k;
+  }
+  for (size_t t = 0; t < q.n_tb; ++t) {
+    const TbDesc& d = q.tbs[t];
+    if (d.n_cb < 1 || d.first_cb < 0 || static_cast<size_t>(d.first_cb) + d.n_cb > q.n_cb || d.tbs < 1)
+      throw InvalidArgument("invalid transport block descriptor");
+    int64_t payload = 0;
+    for (int r = 0; r < d.n_cb; ++r) {
+      const auto& c = q.cbs[d.first_cb + r];
+      payload += c.k - c.filler - (d.n_cb > 1 ? 24 : 0);
+    }
+    if (payload != d.tbs + 24)
+      throw InvalidArgument("code blocks do not add up to TBS + 24 (segmentation mismatch)");
+    if (d.bits_offset < 0 || static_cast<size_t>(d.bits_offset + d.tbs) > q.bits_len)
+      throw InvalidArgument("transport block bits out of range");
+    tbs[t] = DevTb{d.first_cb, d.n_cb, d.tbs, d.bits_offset};
+    bits_len = std::max<int64_t>(bits_len, d.bits_offset + d.tbs);
+  }
+  if (q.n_tb == 0) return;
+  // ---- device buffers ----
+  const float* e_llr = q.e_llr;
+  if (!q.device_memory) {
+    float* de = grow<float>(d_e_llr_, q.e_len);
+    check(cudaMemcpyAsync(de, q.e_llr, q.e_len * sizeof(float), cudaMemcpyHostToDevice, st),
+          "copy rate-matched LLRs in");
+    e_llr = de;
+  }
+  float* d012 = grow<float>(d_d012_, static_cast<size_t>(llr_len));
+  float* post = grow<float>(d_tbpost_, static_cast<size_t>(post_len));
+  uint8_t* bits = q.device_memory ? q.bits : grow<uint8_t>(d_tbbits_, q.bits_len);
+  uint8_t* tb_ok = q.device_memory && q.tb_crc_ok ? q.tb_crc_ok : grow<uint8_t>(d_tbok_, q.n_tb);
+  uint8_t* cb_ok = q.device_memory && q.cb_crc_ok ? q.cb_crc_ok : grow<uint8_t>(d_cbok_, q.n_cb);
+  uint32_t* iters = q.device_memory && q.iterations_used ? q.iterations_used
+                                                         : grow<uint32_t>(d_tbiters_, q.n_cb);
+  DevTb* dtb = grow<DevTb>(d_tb_, q.n_tb);
+  if (d_xpow_a_.bytes == 0) {
+    const auto xa = xpow_table(CrcKind::Crc24A, 6144 * 17);  // > largest TB + CRC24A
+    const auto xb = xpow_table(CrcKind::Crc24B, 6144);
+    d_xpow_a_.reserve(xa.size() * 4);
+    check(cudaMemcpy(d_xpow_a_.ptr, xa.data(), xa.size() * 4, cudaMemcpyHostToDevice), "upload crc");
+  }
+  for (size_t t = 0; t < q.n_tb; ++t)
+    if (tbs[t].tbs + 24 > static_cast<int64_t>(d_xpow_a_.bytes / 4))
+      throw CapacityExceeded("transport block larger than 104424 bits");
+  // ---- de-rate matching, decoding, transport-block finish ----
+  derate_device(q.n_cb, rm.data(), e_llr, q.e_len, d012, static_cast<size_t>(llr_len), st);
+  DecodeRequest rq = q.decode;
+  rq.n_cb = q.n_cb;
+  rq.cbs = cbs.data();
+  rq.llr_len = static_cast<size_t>(llr_len);
+  rq.llr = d012;
+  rq.post_len = static_cast<size_t>(post_len);
+  rq.posterior = post;
+  rq.crc_ok = nullptr;
+  rq.iterations_used = iters;
+  rq.device_memory = true;
+  rq.stream = st;
+  rq.graph = false;
+  if (rq.persistent) decode_persistent(rq); else decode_plain(rq);
+  // decode_* chained its own completion event; the finish kernel follows on the same stream
+  upload(dtb, tbs.data(), q.n_tb * sizeof(DevTb), st);
+  tb_finish_kernel<<<static_cast<unsigned>((q.n_tb * 32 + 255) / 256), 256, 0, st>>>(
+      dtb, static_cast<int>(q.n_tb), static_cast<const DevCb*>(d_cbs_.ptr), post,
+      static_cast<const uint32_t*>(d_xpow_a_.ptr), static_cast<const uint32_t*>(d_xpow_.ptr), bits,
+      tb_ok, cb_ok);
+  check(cudaGetLastError(), "finish launch");
+  timing_.launches += 1;
+  if (!q.device_memory) {
+    check(cudaMemcpyAsync(q.bits, bits, static_cast<size_t>(bits_len), cudaMemcpyDeviceToHost, st),
+          "copy bits out");
+    if (q.tb_crc_ok) check(cudaMemcpyAsync(q.tb_crc_ok, tb_ok, q.n_tb, cudaMemcpyDeviceToHost, st), "copy");
+    if (q.cb_crc_ok) check(cudaMemcpyAsync(q.cb_crc_ok, cb_ok, q.n_cb, cudaMemcpyDeviceToHost, st), "copy");
+    if (q.iterations_used)
+      check(cudaMemcpyAsync(q.iterations_used, iters, q.n_cb * 4, cudaMemcpyDeviceToHost, st), "copy");
+    if (q.posterior)
+      check(cudaMemcpyAsync(q.posterior, post, static_cast<size_t>(post_len) * 4,
+                            cudaMemcpyDeviceToHost, st), "copy");
+  } else if (q.posterior) {
+    check(cudaMemcpyAsync(q.posterior, post, static_cast<size_t>(post_len) * 4,
+                          cudaMemcpyDeviceToDevice, st), "copy");
+  }
+  mark_done(st);
+  if (!q.device_memory) {
+    check(cudaStreamSynchronize(st), "sync");
+    if (rq.persistent) take_error();
+  }
+}
+
+}  // namespace tcb

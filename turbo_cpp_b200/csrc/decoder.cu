@@ -33,14 +33,6 @@ void check(cudaError_t e, const char* what) {
 
 }  // namespace
 
-template <class T>
-T* Decoder::grow(DeviceBuffer& b, size_t count) {
-  void* before = b.ptr;
-  b.reserve(count * sizeof(T));
-  if (b.ptr != before) ++generation_;  // cached graphs hold the old addresses
-  return static_cast<T*>(b.ptr);
-}
-
 void Decoder::upload(void* dst, const void* src, size_t bytes, void* stream) {
   if (bytes == 0) return;
   const size_t padded = (bytes + 255) & ~size_t{255};
@@ -163,7 +155,9 @@ Decoder::~Decoder() {
   if (stream_) cudaStreamDestroy(static_cast<cudaStream_t>(stream_));
   for (DeviceBuffer* b : {&d_perm_, &d_inv_, &d_xpow_, &d_cbs_, &d_wincb_, &d_start_, &d_llr_,
                           &d_sysi_, &d_e1i_, &d_e2_, &d_post_, &d_seed_, &d_done_, &d_iters_,
-                          &d_crc_, &d_ckpt_})
+                          &d_crc_, &d_ckpt_, &d_tasks_, &d_queue_, &d_rm_, &d_e_llr_, &d_d012_,
+                          &d_tbpost_, &d_tbbits_, &d_tbok_, &d_cbok_, &d_tbiters_, &d_tb_,
+                          &d_xpow_a_})
     b->release();
 }
 

@@ -67,6 +67,44 @@ struct DecodeRequest {
   void* stream = nullptr;
 };
 
+// One code block of the transport-block chain: its rate-matched LLRs (E of them at e_offset)
+// and where its de-rate-matched [d0|d1|d2] go (llr_offset, multiple of 4 floats).
+struct RmBlockDesc {
+  int32_t k;
+  int32_t filler;
+  int32_t e;
+  uint32_t rv;
+  int64_t e_offset;
+  int64_t llr_offset;
+};
+
+// One transport block: its code blocks are [first_cb, first_cb + n_cb); its TBS decoded bits
+// go to bits_offset.
+struct TbDesc {
+  int64_t tbs;
+  int32_t first_cb;
+  int32_t n_cb;
+  int64_t bits_offset;
+};
+
+struct TbRequest {
+  size_t n_tb = 0;
+  const TbDesc* tbs = nullptr;        // host
+  size_t n_cb = 0;
+  const RmBlockDesc* cbs = nullptr;   // host; llr_offset ignored (laid out internally)
+  size_t e_len = 0;
+  const float* e_llr = nullptr;
+  size_t bits_len = 0;
+  uint8_t* bits = nullptr;            // one byte per decoded bit
+  uint8_t* tb_crc_ok = nullptr;       // n_tb
+  uint8_t* cb_crc_ok = nullptr;       // n_cb
+  uint32_t* iterations_used = nullptr;  // n_cb
+  float* posterior = nullptr;         // optional: sum K, blocks back to back
+  bool device_memory = false;
+  void* stream = nullptr;
+  DecodeRequest decode;               // iterations, early stop, schedule, window, guard, scales
+};
+
 struct DeviceBuffer {
   void* ptr = nullptr;
   size_t bytes = 0;
@@ -108,6 +146,11 @@ class Decoder {
   void load_tuning(const std::string& path);
   static std::string signature(const DecodeRequest& rq);
   Timing timing(bool reset);  // waits for the recorded events
+
+  // transport-block chain on the device (chain.cu)
+  void derate_match_llr(size_t n, const RmBlockDesc* blocks, const float* e_llr, size_t e_len,
+                        float* d012, size_t llr_len, void* stream);
+  void decode_transport_blocks(const TbRequest& q);
   int sm_count() const { return sm_count_; }
 
  private:
@@ -118,7 +161,14 @@ class Decoder {
   // host -> device copy of launch descriptors; while capturing, from graph-owned pinned memory
   void upload(void* dst, const void* src, size_t bytes, void* stream);
   template <class T>
-  T* grow(DeviceBuffer& b, size_t count);
+  T* grow(DeviceBuffer& b, size_t count) {
+    void* before = b.ptr;
+    b.reserve(count * sizeof(T));
+    if (b.ptr != before) ++generation_;  // cached graphs hold the old addresses
+    return static_cast<T*>(b.ptr);
+  }
+  void derate_device(size_t n, const RmBlockDesc* blocks, const float* e_llr, size_t e_len,
+                     float* d012, size_t llr_len, void* stream);
 
   // CUDA graphs of previously seen device-memory requests (same shapes, pointers, options)
   struct GraphEntry {
@@ -158,6 +208,8 @@ class Decoder {
   DeviceBuffer d_perm_, d_inv_, d_xpow_;
   DeviceBuffer d_cbs_, d_wincb_, d_start_, d_llr_, d_sysi_, d_e1i_, d_e2_, d_post_, d_seed_,
       d_done_, d_iters_, d_crc_, d_ckpt_, d_tasks_, d_queue_;
+  DeviceBuffer d_rm_, d_e_llr_, d_d012_, d_tbpost_, d_tbbits_, d_tbok_, d_cbok_, d_tbiters_, d_tb_,
+      d_xpow_a_;
   int persist_blocks_per_sm_ = 0;
   DeviceBuffer d_err_;          // sticky: set by a persistent-schedule wait that gave up
   int stall_task_ = -1;
