@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the config-3 (transport-block chain) and config-5 (mixed K) figures")
     return ap.parse_args()
 
 
@@ -244,6 +246,73 @@ def workload_config(args):
         "guard": 96 if args.guard < 0 else args.guard, "ebn0_db": EBN0[:args.points],
         "l2": "inputs 302 MB per step > 126 MB L2 (no flush needed)",
     }
+
+
+def config3_figure(tc, dev, iters):
+    """512 transport blocks of uneven size through the device chain (de-rate matching,
+    persistent decode with CRC24B early stop, CRC24A): info Mbit/s = sum TBS / wall time of the
+    synchronous host-buffer call (host -> device copy of the rate-matched LLRs included)."""
+    from turbo_cpp_b200.workloads import config3_transport_blocks
+
+    tbs, blocks, e_llr, truth, ebs = config3_transport_blocks(512, seed=33)
+    info = sum(t[0] for t in tbs)
+    out = {}
+    for name, sched in (("persistent", tc.SCHEDULE_PERSISTENT), ("plain", tc.SCHEDULE_PLAIN)):
+        o = tc.DecodeOptions(iters, True, 0, -1, sched)
+        dev.decode_tbs(tbs, blocks, e_llr, o)  # warm-up
+        t = time.perf_counter()
+        reps = 3
+        for _ in range(reps):
+            bits, tb_ok, cb_ok, it = dev.decode_tbs(tbs, blocks, e_llr, o)
+        dt = (time.perf_counter() - t) / reps
+        tb_err = sum(not np.array_equal(bits[j], truth[j]) for j in range(len(tbs)))
+        out[name] = {"value": info / dt / 1e6, "unit": "Mbit/s", "ms": dt * 1e3,
+                     "tb_crc_pass": float(np.mean(tb_ok)), "tb_bit_errors_blocks": int(tb_err),
+                     "mean_iterations": float(np.mean(it))}
+    out["workload"] = (f"{len(tbs)} TBs, TBS ~ U(multiples of 8 in [1000, 97896]) (stand-in for "
+                       f"the 36.213 table), {len(blocks)} code blocks, r ~ U[0.3,0.9], Eb/N0 ~ "
+                       f"U[0.5,3.0] dB per TB, 8 max iterations, CRC24B early stop; host LLRs in, "
+                       f"host bits out")
+    return out
+
+
+def config5_figure(tc, dev, stream, iters):
+    """20000 code blocks, K from all 188 sizes with P ~ K, CRC24B payloads, Eb/N0 ~ U[0, 2] dB,
+    early stop, one persistent launch: device-resident info Mbit/s (K-24 per block)."""
+    import torch
+    from turbo_cpp_b200.workloads import config5_code_blocks
+
+    ks, llr, bits, eb = config5_code_blocks(20000, seed=55)
+    cbs, llr_len, post_len = tc.Decoder.layout(ks)
+    x = torch.from_numpy(llr).cuda()
+    post = torch.empty(post_len, dtype=torch.float32, device="cuda")
+    itd = torch.zeros(ks.size, dtype=torch.int32, device="cuda")
+    info = int(np.sum(ks - 24))
+    out = {}
+    for name, sched in (("persistent", tc.SCHEDULE_PERSISTENT), ("plain", tc.SCHEDULE_PLAIN)):
+        o = tc.DecodeOptions(iters, True, 0, -1, sched)
+        dev.decode_device(cbs, ks.size, x.data_ptr(), llr_len, post.data_ptr(), post_len, 0,
+                          itd.data_ptr(), options=o, stream=stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            dev.decode_device(cbs, ks.size, x.data_ptr(), llr_len, post.data_ptr(), post_len, 0,
+                              itd.data_ptr(), options=o, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        p = post.cpu().numpy()
+        errs = (p >= 0) != bits
+        starts = np.concatenate([[0], np.cumsum(ks)[:-1]])
+        blk = np.logical_or.reduceat(errs, starts)
+        sel = (eb > 0.5) & (eb < 0.7)
+        out[name] = {"value": info / ms / 1e3, "unit": "Mbit/s", "ms": ms,
+                     "mean_iterations": float(itd.float().mean().item()),
+                     "bler": float(blk.mean()), "bler_0.5_0.7dB": float(blk[sel].mean())}
+    out["workload"] = ("20000 code blocks, K over all 188 QPP sizes with P ~ K, K-24 payload + "
+                       "CRC24B, Eb/N0 ~ U[0,2] dB per block, 8 max iterations, CRC24B early "
+                       "stop, device-resident LLRs")
+    return out
 
 
 def ber_bler(post, bits, n, k):
@@ -433,6 +502,11 @@ def main():
         line["autotune"] = tuned
     if e2e:
         line["e2e"] = e2e
+    # ---- config 3 (transport-block chain) and config 5 (mixed K, early stop) figures ----
+    if not args.no_configs:
+        line["config3_chain"] = config3_figure(tc, dev, it)
+        line["config5_mixed"] = config5_figure(tc, dev, stream, it)
+
     # ---- plain per-block GPU path: one code block per call, as the reference API decodes ----
     per_block = []
     sub = batches[3 % len(batches)].cpu().numpy()[:8 * 3 * (K + 4)]
