@@ -80,6 +80,11 @@ class Oracle(_Lib):
         _sig(L, "or_decode_batch", None, batch_args + [_i32p, _i32p, C.c_int32])
         _sig(L, "or_decode_batch_windowed", None,
              batch_args + [C.c_int32, C.c_int32, _i32p, _i32p, C.c_int32])
+        _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+        _f64n = C.POINTER(C.c_double)
+        _sig(L, "or_adj_seed_count", C.c_int64, [C.c_int32, C.c_int32, C.c_int32])
+        _sig(L, "or_adj_vjp", None,
+             [C.c_int32, _f64p, C.c_int32, _f64p, C.c_int32, C.c_int32] + [_f64n] * 6)
 
     # -- QPP --
     def qpp_table(self):
@@ -162,6 +167,26 @@ class Oracle(_Lib):
             self.lib.or_decode_cb(k, filler, llr, iters, int(early_stop), post, C.byref(ok),
                                   C.byref(used))
         return post, bool(ok.value), used.value
+
+    # -- FP64 differentiable decoder (scaled extrinsics, windowed schedule) and its adjoint --
+    def adj_vjp(self, k, llr, scales, window=0, guard=0, grad_post=None, frozen_seeds=None):
+        """Returns (posterior, seeds used, grad_llr, grad_scales); the gradients are the
+        vector-Jacobian product with grad_post (None: forward only, gradients None).
+        len(scales) // 2 iterations."""
+        def ptr(a):
+            return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+        scales = np.ascontiguousarray(scales, np.float64)
+        iters = scales.size // 2
+        llr = np.ascontiguousarray(llr, np.float64)
+        post = np.empty(k, np.float64)
+        seeds = np.empty(self.lib.or_adj_seed_count(k, iters, window), np.float64)
+        fz = None if frozen_seeds is None else np.ascontiguousarray(frozen_seeds, np.float64)
+        gp = None if grad_post is None else np.ascontiguousarray(grad_post, np.float64)
+        g_llr = np.empty(3 * (k + 4), np.float64) if gp is not None else None
+        g_s = np.empty(scales.size, np.float64) if gp is not None else None
+        self.lib.or_adj_vjp(k, llr, iters, scales, window, guard, ptr(fz), ptr(gp), ptr(post),
+                            ptr(g_llr), ptr(g_s), ptr(seeds))
+        return post, seeds, g_llr, g_s
 
     def decode_batch(self, ks, fillers, llr, llr_off, out_off, iters=8, early_stop=False,
                      window=0, guard=0, threads=0):

@@ -694,3 +694,354 @@ void or_decode_batch_windowed(int32_t n, const int32_t* k, const int32_t* filler
                window, guard, crc_ok, iterations_used, 0};
   run_batch(&b, threads);
 }
+
+/* ------------------------------------------------------------------------------------------ */
+/* FP64 differentiable decoder and its hand-written adjoint                                    */
+/* ------------------------------------------------------------------------------------------ */
+/*
+ * The differentiated function: the windowed schedule of decode_common (window W, guard G,
+ * next-iteration-initialisation seeds) in natural-log FP64, no early stop, the extrinsic of SISO
+ * j (j = 2*it upper, 2*it+1 lower) multiplied by scales[j] before it becomes the other SISO's
+ * a-priori and enters the posterior Ls + e1 + e2.  The seeds are constants of the function (the
+ * gradient stops at them); with W >= K there are none and this is the reference's full-trellis
+ * decoder (turbo_decode_code_block_cpu, lte_turbo.cpp:736-813) with the scales inserted.
+ * Per-step normalisations subtract a common value from all 8 metrics; every extrinsic is a
+ * difference of two log-sums over the same metrics, so they are constants of the function too.
+ */
+static double lse2(double x, double y) {
+  if (x == -INFINITY) return y;
+  if (y == -INFINITY) return x;
+  const double m = x > y ? x : y;
+  return m + log1p(exp(-fabs(x - y)));
+}
+
+/* branch metric (u ? a : -a) + (p ? b : -b), a = (Ls+La)/2, b = Lp/2 (lte_turbo.cpp:437-438) */
+static inline double gam(const trellis_t* T, int s, int u, double a, double b) {
+  return (u ? a : -a) + (T->parity[s][u] ? b : -b);
+}
+
+/* beta at the block end from the three termination steps (lte_turbo.cpp:357-378), and its
+ * derivatives w.r.t. the tail systematic (ts) and parity (tp) LLRs */
+static void tail_beta64(const double ts[3], const double tp[3], double beta[8], double dts[8][3],
+                        double dtp[8][3]) {
+  for (int s = 0; s < 8; ++s) {
+    uint8_t cur = (uint8_t)s, in[3];
+    termination(cur, in);
+    double m = 0.0;
+    for (int i = 0; i < 3; ++i) {
+      uint8_t p, n;
+      rsc_step(cur, in[i], &p, &n);
+      cur = n;
+      dts[s][i] = in[i] ? 0.5 : -0.5;
+      dtp[s][i] = p ? 0.5 : -0.5;
+      m += dts[s][i] * ts[i] + dtp[s][i] * tp[i];
+    }
+    beta[s] = m;
+  }
+}
+
+/* one window: alpha over positions [a_lo, hi] from a_in (NULL: the start state), beta over
+ * [lo, b_hi] from b_in (NULL: the tail metric), extrinsic over [lo, hi) */
+typedef struct {
+  int32_t a_lo, lo, hi, b_hi;
+  int start, tail; /* edge metric used instead of a seed */
+} seg64_t;
+
+static seg64_t seg64(int32_t k, int32_t W, int32_t G, int32_t w) {
+  seg64_t g;
+  g.lo = w * W;
+  g.hi = g.lo + W < k ? g.lo + W : k;
+  g.a_lo = g.lo - G;
+  g.b_hi = g.hi + G;
+  g.start = g.a_lo <= 0;
+  g.tail = g.b_hi >= k;
+  if (g.start) g.a_lo = 0;
+  if (g.tail) g.b_hi = k;
+  return g;
+}
+
+static void seg64_forward(const trellis_t* T, const double* sys, const double* par,
+                          const double* apr, seg64_t g, const double* a_in, const double* b_in,
+                          const double ts[3], const double tp[3], double* alpha, double* beta,
+                          double* ext) {
+  for (int s = 0; s < 8; ++s) alpha[s] = a_in ? a_in[s] : (s == 0 ? 0.0 : -INFINITY);
+  for (int32_t p = g.a_lo; p < g.hi; ++p) {
+    const double a = 0.5 * (sys[p] + apr[p]), b = 0.5 * par[p];
+    const double* at = alpha + 8 * (p - g.a_lo);
+    double* an = alpha + 8 * (p + 1 - g.a_lo);
+    for (int s = 0; s < 8; ++s) an[s] = -INFINITY;
+    for (int s = 0; s < 8; ++s)
+      for (int u = 0; u < 2; ++u) {
+        const int n = T->next[s][u];
+        an[n] = lse2(an[n], at[s] + gam(T, s, u, a, b));
+      }
+    const double c = an[0];
+    for (int s = 0; s < 8; ++s) an[s] -= c;
+  }
+  double* bk = beta + 8 * (g.b_hi - g.lo);
+  if (b_in) {
+    for (int s = 0; s < 8; ++s) bk[s] = b_in[s];
+  } else {
+    double dts[8][3], dtp[8][3];
+    tail_beta64(ts, tp, bk, dts, dtp);
+  }
+  for (int32_t p = g.b_hi; p-- > g.lo;) {
+    const double a = 0.5 * (sys[p] + apr[p]), b = 0.5 * par[p];
+    const double* bn = beta + 8 * (p + 1 - g.lo);
+    double* bt = beta + 8 * (p - g.lo);
+    for (int s = 0; s < 8; ++s) {
+      bt[s] = -INFINITY;
+      for (int u = 0; u < 2; ++u) bt[s] = lse2(bt[s], bn[T->next[s][u]] + gam(T, s, u, a, b));
+    }
+    const double c = bt[0];
+    for (int s = 0; s < 8; ++s) bt[s] -= c;
+  }
+  for (int32_t p = g.lo; p < g.hi; ++p) {
+    const double b = 0.5 * par[p];
+    const double* at = alpha + 8 * (p - g.a_lo);
+    const double* bn = beta + 8 * (p + 1 - g.lo);
+    double l[2] = {-INFINITY, -INFINITY};
+    for (int s = 0; s < 8; ++s)
+      for (int u = 0; u < 2; ++u)
+        l[u] = lse2(l[u], at[s] + bn[T->next[s][u]] + (T->parity[s][u] ? b : -b));
+    ext[p] = l[1] - l[0];
+  }
+}
+
+/* Adjoint of seg64_forward: g_ext over [lo, hi) in, accumulates d/d(Ls+La) and d/d(Lp) over
+ * [a_lo, b_hi) and, when the tail metric was used, d/d ts and d/d tp.  Reverse mode through
+ * the softmax weights of every log-sum; alpha/beta as seg64_forward left them. */
+static void seg64_adjoint(const trellis_t* T, const double* sys, const double* par,
+                          const double* apr, seg64_t g, const double ts[3], const double tp[3],
+                          const double* alpha, const double* beta, const double* g_ext,
+                          double* g_sa, double* g_par, double g_ts[3], double g_tp[3]) {
+  const int32_t na = g.hi - g.a_lo + 1, nb = g.b_hi - g.lo + 1;
+  double* ab = (double*)calloc(8u * (size_t)na, sizeof(double));
+  double* bb = (double*)calloc(8u * (size_t)nb, sizeof(double));
+  for (int32_t p = g.lo; p < g.hi; ++p) { /* extrinsic = LSE1 - LSE0 */
+    const double b = 0.5 * par[p];
+    const double* at = alpha + 8 * (p - g.a_lo);
+    const double* bn = beta + 8 * (p + 1 - g.lo);
+    double m[8][2], l[2] = {-INFINITY, -INFINITY};
+    for (int s = 0; s < 8; ++s)
+      for (int u = 0; u < 2; ++u) {
+        m[s][u] = at[s] + bn[T->next[s][u]] + (T->parity[s][u] ? b : -b);
+        l[u] = lse2(l[u], m[s][u]);
+      }
+    for (int s = 0; s < 8; ++s)
+      for (int u = 0; u < 2; ++u) {
+        if (m[s][u] == -INFINITY) continue;
+        const double v = exp(m[s][u] - l[u]) * (u ? 1.0 : -1.0) * g_ext[p];
+        ab[8 * (p - g.a_lo) + s] += v;
+        bb[8 * (p + 1 - g.lo) + T->next[s][u]] += v;
+        g_par[p] += 0.5 * v * (T->parity[s][u] ? 1.0 : -1.0);
+      }
+  }
+  for (int32_t p = g.lo; p < g.b_hi; ++p) { /* beta_p = LSE_u(beta_{p+1}[n] + gamma), forward */
+    const double a = 0.5 * (sys[p] + apr[p]), b = 0.5 * par[p];
+    const double* bn = beta + 8 * (p + 1 - g.lo);
+    for (int s = 0; s < 8; ++s) {
+      const double gs = bb[8 * (p - g.lo) + s];
+      if (gs == 0.0) continue;
+      double v[2], l = -INFINITY;
+      for (int u = 0; u < 2; ++u) {
+        v[u] = bn[T->next[s][u]] + gam(T, s, u, a, b);
+        l = lse2(l, v[u]);
+      }
+      for (int u = 0; u < 2; ++u) {
+        const double q = exp(v[u] - l) * gs;
+        bb[8 * (p + 1 - g.lo) + T->next[s][u]] += q;
+        g_sa[p] += 0.5 * q * (u ? 1.0 : -1.0);
+        g_par[p] += 0.5 * q * (T->parity[s][u] ? 1.0 : -1.0);
+      }
+    }
+  }
+  for (int32_t p = g.hi; p-- > g.a_lo;) { /* alpha_{p+1}[n] = LSE over (s,u)->n, backward */
+    const double a = 0.5 * (sys[p] + apr[p]), b = 0.5 * par[p];
+    const double* at = alpha + 8 * (p - g.a_lo);
+    double l[8];
+    for (int n = 0; n < 8; ++n) l[n] = -INFINITY;
+    for (int s = 0; s < 8; ++s)
+      for (int u = 0; u < 2; ++u)
+        l[T->next[s][u]] = lse2(l[T->next[s][u]], at[s] + gam(T, s, u, a, b));
+    for (int s = 0; s < 8; ++s)
+      for (int u = 0; u < 2; ++u) {
+        const int n = T->next[s][u];
+        const double gn = ab[8 * (p + 1 - g.a_lo) + n];
+        if (gn == 0.0 || at[s] == -INFINITY) continue;
+        const double v = exp(at[s] + gam(T, s, u, a, b) - l[n]) * gn;
+        ab[8 * (p - g.a_lo) + s] += v;
+        g_sa[p] += 0.5 * v * (u ? 1.0 : -1.0);
+        g_par[p] += 0.5 * v * (T->parity[s][u] ? 1.0 : -1.0);
+      }
+  }
+  if (g.tail) {
+    double bk[8], dts[8][3], dtp[8][3];
+    tail_beta64(ts, tp, bk, dts, dtp);
+    for (int s = 0; s < 8; ++s)
+      for (int i = 0; i < 3; ++i) {
+        g_ts[i] += bb[8 * (nb - 1) + s] * dts[s][i];
+        g_tp[i] += bb[8 * (nb - 1) + s] * dtp[s][i];
+      }
+  }
+  free(ab);
+  free(bb);
+}
+
+static int32_t adj_window(int32_t k, int32_t window) {
+  return (window <= 0 || window > k) ? k : window;
+}
+
+int64_t or_adj_seed_count(int32_t k, int32_t iters, int32_t window) {
+  const int32_t W = adj_window(k, window);
+  return (int64_t)2 * iters * ((k + W - 1) / W) * 16;
+}
+
+/* tail LLRs of both SISOs (gather_tails, lte_turbo.cpp:758-773) and where they come from in
+ * [d0|d1|d2] (offsets into the 3(K+4) LLRs) */
+static void tails64(int32_t k, const double* llr, double ts[2][3], double tp[2][3],
+                    int32_t its[2][3], int32_t itp[2][3]) {
+  const int32_t o0 = 0, o1 = k + 4, o2 = 2 * (k + 4);
+  const int32_t s_idx[2][3] = {{o0 + k, o0 + k + 2, -1}, {o1 + k + 3, o2 + k, o2 + k + 2}};
+  const int32_t p_idx[2][3] = {{o1 + k, o0 + k + 1, o1 + k + 2}, {o2 + k + 1, o0 + k + 3, o2 + k + 3}};
+  for (int h = 0; h < 2; ++h)
+    for (int i = 0; i < 3; ++i) {
+      its[h][i] = s_idx[h][i];
+      itp[h][i] = p_idx[h][i];
+      ts[h][i] = s_idx[h][i] >= 0 ? llr[s_idx[h][i]] : 0.0;
+      tp[h][i] = llr[p_idx[h][i]];
+    }
+}
+
+void or_adj_vjp(int32_t k, const double* llr, int32_t iters, const double* scales,
+                int32_t window, int32_t guard, const double* frozen_seeds,
+                const double* grad_post, double* posterior, double* grad_llr,
+                double* grad_scales, double* seeds_out) {
+  const trellis_t T = make_trellis();
+  const int32_t W = adj_window(k, window);
+  const int32_t G = guard < 0 ? 0 : (guard > W ? W : guard);
+  const int32_t nw = (k + W - 1) / W, nj = 2 * iters;
+  const double* d0 = llr;
+  const double* d1 = llr + (k + 4);
+  const double* d2 = llr + 2 * (k + 4);
+  double ts[2][3], tp[2][3];
+  int32_t its[2][3], itp[2][3];
+  tails64(k, llr, ts, tp, its, itp);
+  int32_t* perm = (int32_t*)malloc(sizeof(int32_t) * (size_t)k);
+  or_qpp_perm(k, perm);
+  const size_t rows = (size_t)(W + 2 * G + 1);
+  double* alpha = (double*)malloc(sizeof(double) * 8u * rows);
+  double* beta = (double*)malloc(sizeof(double) * 8u * rows);
+  double* sys_i = (double*)malloc(sizeof(double) * (size_t)k);
+  double* e1 = (double*)calloc((size_t)k, sizeof(double));
+  double* e2 = (double*)calloc((size_t)k, sizeof(double));
+  double* x = (double*)malloc(sizeof(double) * (size_t)k);
+  /* tape: a-priori and extrinsic (unscaled) per SISO, seeds per SISO and window */
+  double* tape_apr = (double*)malloc(sizeof(double) * (size_t)k * (size_t)nj);
+  double* tape_x = (double*)malloc(sizeof(double) * (size_t)k * (size_t)nj);
+  double* seeds = (double*)calloc((size_t)(nj + 2) * (size_t)nw * 16u, sizeof(double));
+  for (int32_t i = 0; i < k; ++i) sys_i[i] = d0[perm[i]];
+  for (int32_t it = 0; it < iters; ++it)
+    for (int h = 0; h < 2; ++h) {
+      const int j = 2 * it + h;
+      const double* sys = h ? sys_i : d0;
+      const double* par = h ? d2 : d1;
+      double* apr = tape_apr + (size_t)j * k;
+      if (h)
+        for (int32_t i = 0; i < k; ++i) apr[i] = e1[perm[i]];
+      else
+        memcpy(apr, e2, sizeof(double) * (size_t)k);
+      double* sj = frozen_seeds ? (double*)frozen_seeds + (size_t)j * nw * 16
+                                : seeds + (size_t)j * nw * 16;
+      double* snext = seeds + (size_t)(j + 2) * nw * 16;
+      for (int32_t w = 0; w < nw; ++w) {
+        const seg64_t g = seg64(k, W, G, w);
+        seg64_forward(&T, sys, par, apr, g, g.start ? NULL : sj + 16 * w,
+                      g.tail ? NULL : sj + 16 * w + 8, ts[h], tp[h], alpha, beta, x);
+        /* next-iteration seeds: alpha at hi-G for window w+1, beta at lo+G for window w-1 */
+        if (w + 1 < nw && g.hi - G > 0)
+          memcpy(snext + 16 * (w + 1), alpha + 8 * (g.hi - G - g.a_lo), 8 * sizeof(double));
+        if (w > 0 && g.lo + G < k)
+          memcpy(snext + 16 * (w - 1) + 8, beta + 8 * (g.lo + G - g.lo), 8 * sizeof(double));
+      }
+      memcpy(tape_x + (size_t)j * k, x, sizeof(double) * (size_t)k);
+      if (h)
+        for (int32_t i = 0; i < k; ++i) e2[perm[i]] = scales[j] * x[i];
+      else
+        for (int32_t i = 0; i < k; ++i) e1[i] = scales[j] * x[i];
+    }
+  if (seeds_out) {
+    if (frozen_seeds)
+      memcpy(seeds_out, frozen_seeds, sizeof(double) * (size_t)nj * nw * 16);
+    else
+      memcpy(seeds_out, seeds, sizeof(double) * (size_t)nj * nw * 16);
+  }
+  if (posterior)
+    for (int32_t i = 0; i < k; ++i) posterior[i] = d0[i] + e1[i] + e2[i];
+
+  if (grad_post) {
+    const double* sd = frozen_seeds ? frozen_seeds : seeds;
+    memset(grad_llr, 0, sizeof(double) * 3u * (size_t)(k + 4));
+    memset(grad_scales, 0, sizeof(double) * (size_t)nj);
+    double* g0 = grad_llr;
+    double* g1 = grad_llr + (k + 4);
+    double* g2 = grad_llr + 2 * (k + 4);
+    double* ge1 = (double*)calloc((size_t)k, sizeof(double)); /* d/d e1, natural order */
+    double* ge2 = (double*)calloc((size_t)k, sizeof(double)); /* d/d e2, natural order */
+    double* gx = (double*)malloc(sizeof(double) * (size_t)k);
+    double* gsa = (double*)malloc(sizeof(double) * (size_t)k);
+    double* gpar = (double*)malloc(sizeof(double) * (size_t)k);
+    for (int32_t i = 0; i < k; ++i) { /* posterior = Ls + e1 + e2 */
+      g0[i] += grad_post[i];
+      ge1[i] = grad_post[i];
+      ge2[i] = grad_post[i];
+    }
+    for (int32_t it = iters; it-- > 0;)
+      for (int h = 1; h >= 0; --h) {
+        const int j = 2 * it + h;
+        const double* X = tape_x + (size_t)j * k;
+        const double* sys = h ? sys_i : d0;
+        const double* par = h ? d2 : d1;
+        const double* apr = tape_apr + (size_t)j * k;
+        for (int32_t i = 0; i < k; ++i) { /* e = scale * x, lower in interleaved order */
+          const double ge = h ? ge2[perm[i]] : ge1[i];
+          grad_scales[j] += ge * X[i];
+          gx[i] = ge * scales[j];
+        }
+        memset(gsa, 0, sizeof(double) * (size_t)k);
+        memset(gpar, 0, sizeof(double) * (size_t)k);
+        double gts[3] = {0, 0, 0}, gtp[3] = {0, 0, 0};
+        const double* sj = sd + (size_t)j * nw * 16;
+        for (int32_t w = 0; w < nw; ++w) {
+          const seg64_t g = seg64(k, W, G, w);
+          seg64_forward(&T, sys, par, apr, g, g.start ? NULL : sj + 16 * w,
+                        g.tail ? NULL : sj + 16 * w + 8, ts[h], tp[h], alpha, beta, x);
+          seg64_adjoint(&T, sys, par, apr, g, ts[h], tp[h], alpha, beta, gx, gsa, gpar, gts,
+                        gtp);
+        }
+        for (int i = 0; i < 3; ++i) {
+          if (its[h][i] >= 0) grad_llr[its[h][i]] += gts[i];
+          grad_llr[itp[h][i]] += gtp[i];
+        }
+        if (h) { /* sys_i[i] = d0[perm[i]], a-priori[i] = e1[perm[i]] */
+          for (int32_t i = 0; i < k; ++i) {
+            g0[perm[i]] += gsa[i];
+            g2[i] += gpar[i];
+          }
+          memset(ge1, 0, sizeof(double) * (size_t)k); /* e1 of iteration it: only via this SISO */
+          if (it + 1 == iters)
+            for (int32_t i = 0; i < k; ++i) ge1[i] = grad_post[i];
+          for (int32_t i = 0; i < k; ++i) ge1[perm[i]] += gsa[i];
+        } else { /* a-priori = e2 of iteration it-1 (zero for it = 0) */
+          for (int32_t i = 0; i < k; ++i) {
+            g0[i] += gsa[i];
+            g1[i] += gpar[i];
+            ge2[i] = gsa[i];
+          }
+        }
+      }
+    free(ge1); free(ge2); free(gx); free(gsa); free(gpar);
+  }
+  free(perm); free(alpha); free(beta); free(sys_i); free(e1); free(e2); free(x);
+  free(tape_apr); free(tape_x); free(seeds);
+}

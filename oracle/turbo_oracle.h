@@ -90,6 +90,22 @@ void or_decode_batch_windowed(int32_t n, const int32_t* k, const int32_t* filler
                               int32_t window, int32_t guard, int32_t* crc_ok,
                               int32_t* iterations_used, int32_t threads);
 
+/* ---- FP64 differentiable decoder and its adjoint (checker of the GPU adjoint) ----
+ * The windowed schedule of or_decode_cb_windowed (window, guard, next-iteration seeds) in
+ * natural-log FP64, `iters` iterations, no early stop, the extrinsic of SISO j (j = 2*it upper,
+ * 2*it+1 lower) multiplied by scales[j] before it is the other SISO's a-priori and before it
+ * enters the posterior Ls + e1 + e2.  The seeds are constants of the function; window <= 0 or
+ * >= K is the full trellis (no seeds).  Seeds are [2*iters][windows][16] (alpha 0..7, beta
+ * 8..15, the values SISO j used in window w).  frozen_seeds (may be NULL) replaces the
+ * schedule's own seeds; seeds_out (may be NULL) receives the seeds used.  grad_post (may be
+ * NULL: forward only) is d loss / d posterior; then grad_llr (3(K+4)) and grad_scales
+ * (2*iters) receive the vector-Jacobian product. */
+int64_t or_adj_seed_count(int32_t k, int32_t iters, int32_t window);
+void or_adj_vjp(int32_t k, const double* llr, int32_t iters, const double* scales,
+                int32_t window, int32_t guard, const double* frozen_seeds,
+                const double* grad_post, double* posterior, double* grad_llr,
+                double* grad_scales, double* seeds_out);
+
 #ifdef __cplusplus
 }
 #endif
