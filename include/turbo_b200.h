@@ -236,6 +236,33 @@ typedef struct {
 TC_API int tc_decoder_set_timing(tc_decoder* dec, int enable);
 TC_API int tc_decoder_timing(tc_decoder* dec, tc_timing* out, int reset);
 
+/* ---------------- differentiable decoder and its adjoint (new) ----------------
+ * No counterpart in the reference, which has no gradient code; the forward function is the
+ * reference decoder (turbo_decode_code_block_cpu, lte_turbo.cpp:736-813) unrolled for
+ * `iterations` iterations without early stop, with the extrinsic of SISO j (j = 2*it upper,
+ * 2*it+1 lower) multiplied by scales[j] before it becomes the other SISO's a-priori and before
+ * it enters the posterior Ls + e1 + e2, run on the windowed schedule (window, guard;
+ * 0 / -1 = 64 / 32; window >= K is the full trellis) whose next-iteration seeds are constants
+ * of the function.  The adjoint is hand-written: alpha checkpointed at the window starts and
+ * every 4 steps, recomputed on the backward pass, the transposed softmax weights of every max*.
+ * All buffers are device memory ordered on `stream` (NULL = the legacy default stream);
+ * `scales` is host memory (2*iterations floats, NULL = all 1).  The LLR buffer must stay
+ * unchanged between a forward pass and its backward pass.  A forward pass returns a tape id;
+ * the backward pass of an older tape (replaced by a later forward pass on the same handle)
+ * fails with TC_ERR_INVALID_ARGUMENT. */
+typedef struct tc_adjoint tc_adjoint;
+TC_API int tc_adjoint_create(tc_decoder* dec, tc_adjoint** out);
+TC_API int tc_adjoint_destroy(tc_adjoint* adj);
+TC_API int tc_adjoint_forward(tc_adjoint* adj, size_t n_cb, const tc_code_block* cbs,
+                              size_t llr_len, const float* llr, size_t post_len, float* posterior,
+                              uint32_t iterations, const float* scales, int32_t window,
+                              int32_t guard, void* stream, uint64_t* tape);
+/* grad_posterior: post_len floats (posterior layout); grad_llr: llr_len floats (LLR layout,
+ * 0 outside every block); grad_scales: 2*iterations floats. */
+TC_API int tc_adjoint_backward(tc_adjoint* adj, uint64_t tape, const float* grad_posterior,
+                               float* grad_llr, float* grad_scales, void* stream);
+TC_API int tc_adjoint_launches(tc_adjoint* adj, uint64_t* launches);
+
 #ifdef __cplusplus
 }
 #endif

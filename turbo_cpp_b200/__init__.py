@@ -138,6 +138,12 @@ _SIGNATURES = {
     "tc_autotune_load": [_VP, C.c_char_p],
     "tc_decoder_set_timing": [_VP, C.c_int],
     "tc_decoder_timing": [_VP, _VP, C.c_int],
+    "tc_adjoint_create": [_VP, _VP],
+    "tc_adjoint_destroy": [_VP],
+    "tc_adjoint_forward": [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, C.c_uint32, _VP, C.c_int32,
+                           C.c_int32, _VP, _VP],
+    "tc_adjoint_backward": [_VP, C.c_uint64, _VP, _VP, _VP, _VP],
+    "tc_adjoint_launches": [_VP, _VP],
 }
 
 
@@ -637,6 +643,56 @@ class Decoder:
         opt, _keep = self._opts(o, MEM_DEVICE, stream)
         _call("tc_decode", self._h, int(n_cb), C.addressof(cbs), int(llr_len), llr_ptr,
               int(post_len), post_ptr, crc_ptr or None, iters_ptr or None, C.addressof(opt))
+
+
+class AdjointDecoder:
+    """The differentiable decoder (tc_adjoint_*): a taped forward pass over ``iterations``
+    unrolled iterations with an extrinsic scale per half-iteration, and the hand-written
+    backward pass (d loss / d LLRs and d loss / d scales from d loss / d posterior).  Device
+    buffers only (e.g. torch tensors' data_ptr()), ordered on ``stream``."""
+
+    def __init__(self, decoder: Decoder):
+        self._dec = decoder  # the tables live in the decoder: keep it alive
+        self._lib = decoder._lib
+        h = C.c_void_p()
+        _call("tc_adjoint_create", decoder._h, C.addressof(h))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.tc_adjoint_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forward(self, cbs, n_cb: int, llr_ptr: int, llr_len: int, post_ptr: int, post_len: int,
+                iterations: int, scales=None, window: int = 0, guard: int = -1,
+                stream: int = 0) -> int:
+        """Decodes and records the tape; returns the tape id for backward()."""
+        sc = None
+        if scales is not None:
+            sc = np.ascontiguousarray(scales, np.float32)
+            if sc.size != 2 * iterations:
+                raise InvalidArgument("scales: two per iteration")
+        tape = C.c_uint64()
+        _call("tc_adjoint_forward", self._h, int(n_cb), C.addressof(cbs), int(llr_len), llr_ptr,
+              int(post_len), post_ptr, int(iterations), None if sc is None else _ptr(sc),
+              int(window), int(guard), stream or None, C.addressof(tape))
+        return tape.value
+
+    def backward(self, tape: int, grad_post_ptr: int, grad_llr_ptr: int, grad_scales_ptr: int,
+                 stream: int = 0) -> None:
+        _call("tc_adjoint_backward", self._h, int(tape), grad_post_ptr, grad_llr_ptr,
+              grad_scales_ptr, stream or None)
+
+    def launches(self) -> int:
+        n = C.c_uint64()
+        _call("tc_adjoint_launches", self._h, C.addressof(n))
+        return n.value
 
 
 _default_decoders: dict = {}

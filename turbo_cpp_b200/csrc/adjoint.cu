@@ -1,0 +1,656 @@
+// adjoint.cu -- the hand-written adjoint of the unrolled, scaled Log-MAP iterations.
+//
+// Forward (taped): the plain decoder's SISO kernel, one launch per half-iteration, with the
+// a-priori input and extrinsic output of every half-iteration kept in its own tape slot (slot j
+// is SISO j's a-priori, slot j+1 its scaled extrinsic; slot 0 is zero) and the seeds of every
+// half-iteration in their own slab (SISO j reads slab j and writes slab j+2).
+//
+// Backward: per half-iteration, last to first, one thread per window of the forward schedule
+// runs the adjoint of its window in three phases (base-2 metrics, as the forward):
+//   A  alpha from the window's forward start (seed or block start) to its end, a checkpoint
+//      every 4 steps;
+//   B  backward in time from the beta start (seed or tail) to the alpha start: beta, stored
+//      every 4 steps; alpha recomputed from its checkpoint 4 steps at a time; the extrinsic's
+//      softmax weights give the direct alpha adjoint and d/d parity; the alpha adjoint
+//      recursion (transposed softmax weights of every max*) runs through the window and on
+//      through the alpha warm-up steps;
+//   C  forward in time from the window start to the beta start: beta recomputed from its
+//      checkpoints 4 steps at a time; the beta adjoint recursion, fed by the extrinsic's
+//      direct beta adjoint, runs through the window and the beta warm-up steps to the tail.
+// Per-step normalisations subtract a common value from all 8 metrics and every extrinsic is a
+// difference of two log-sums over the same metrics, so they are constants of the function and
+// the adjoint ignores them.  A warm-up step of one window is an output step of its neighbour, so
+// each window writes its own steps' gradients and its warm-up gradients to separate arrays; a
+// combine kernel adds the three contributions of every position in a fixed order (the result is
+// deterministic), scatters them to d0/d1/d2 and to the other SISO's a-priori adjoint, and adds
+// the tail gradients.  d loss / d scale_j is the sum of d loss / d e * x over the SISO's
+// positions (x its unscaled extrinsic), reduced per window and then in a fixed order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "adjoint.hpp"
+#include "decode_kernels.cuh"
+#include "decoder.hpp"
+#include "lte_codec.hpp"
+
+namespace tcb {
+namespace {
+
+void ok(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+constexpr int kAdjThreads = 64;
+
+__device__ __forceinline__ float rcp(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Softmax weights of the two terms of max*(x0, x1): 2^(x0 - m), 2^(x1 - m), m = log2(2^x0 + 2^x1).
+__device__ __forceinline__ void pair_weights(float x0, float x1, float& w0, float& w1) {
+  const float e = ex2(-fabsf(x0 - x1));
+  const float r = rcp(1.0f + e);
+  const bool first = x0 >= x1;
+  w0 = first ? r : e * r;
+  w1 = first ? e * r : r;
+}
+
+// d(alpha_{p+1}) -> d(alpha_p): ab += J^T abn, with J the softmax weights of alpha_step at p;
+// ga, gb accumulate d/da and d/db of the step's branch metrics.
+__device__ __forceinline__ void alpha_adjoint(const float (&al)[8], float a, float b,
+                                              const float (&abn)[8], float (&ab)[8], float& ga,
+                                              float& gb) {
+  const float g0 = a + b, g1 = a - b;
+#pragma unroll
+  for (int n = 0; n < 8; ++n) {
+    const int n2 = (n >> 2) & 1, n1 = (n >> 1) & 1, n0 = n & 1;
+    const int u = n2 ^ n1 ^ n0;
+    const int p0 = 2 * (n & 3);
+    const int par0 = n2 ^ n1, par1 = n2 ^ n1 ^ 1;
+    float w0, w1;
+    pair_weights(al[p0] + branch(u, par0, g0, g1), al[p0 + 1] + branch(u, par1, g0, g1), w0, w1);
+    const float q0 = w0 * abn[n], q1 = w1 * abn[n];
+    ab[p0] += q0;
+    ab[p0 + 1] += q1;
+    ga += u ? (q0 + q1) : -(q0 + q1);
+    gb += (par0 ? q0 : -q0) + (par1 ? q1 : -q1);
+  }
+}
+
+// d(beta_p) -> d(beta_{p+1}): bbn += J^T bb, J the softmax weights of beta_step at p (bn holds
+// beta_{p+1}).
+__device__ __forceinline__ void beta_adjoint(const float (&bn)[8], float a, float b,
+                                             const float (&bb)[8], float (&bbn)[8], float& ga,
+                                             float& gb) {
+  const float g0 = a + b, g1 = a - b;
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    const int pa0 = parity(s, 0), pa1 = parity(s, 1);
+    float w0, w1;
+    pair_weights(bn[next_state(s, 0)] + branch(0, pa0, g0, g1),
+                 bn[next_state(s, 1)] + branch(1, pa1, g0, g1), w0, w1);
+    const float q0 = w0 * bb[s], q1 = w1 * bb[s];
+    bbn[next_state(s, 0)] += q0;
+    bbn[next_state(s, 1)] += q1;
+    ga += q1 - q0;
+    gb += (pa0 ? q0 : -q0) + (pa1 ? q1 : -q1);
+  }
+}
+
+// Softmax weights of the two 8-way log-sums of the extrinsic (extrinsic2): w_u[s] is the weight
+// of branch (s, u) in the u-side log-sum.  Returns the base-2 extrinsic when WANT_VALUE.
+template <bool WANT_VALUE>
+__device__ __forceinline__ float ext_weights(const float (&al)[8], const float (&be)[8], float b,
+                                             float (&w0)[8], float (&w1)[8]) {
+  float m0[8], m1[8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    m0[s] = al[s] + be[next_state(s, 0)] + (parity(s, 0) ? b : -b);
+    m1[s] = al[s] + be[next_state(s, 1)] + (parity(s, 1) ? b : -b);
+  }
+  const float x0 = fmaxf(fmaxf(fmaxf(m0[0], m0[1]), fmaxf(m0[2], m0[3])),
+                         fmaxf(fmaxf(m0[4], m0[5]), fmaxf(m0[6], m0[7])));
+  const float x1 = fmaxf(fmaxf(fmaxf(m1[0], m1[1]), fmaxf(m1[2], m1[3])),
+                         fmaxf(fmaxf(m1[4], m1[5]), fmaxf(m1[6], m1[7])));
+  float s0 = 0.0f, s1 = 0.0f;
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    w0[s] = ex2(m0[s] - x0);
+    w1[s] = ex2(m1[s] - x1);
+    s0 += w0[s];
+    s1 += w1[s];
+  }
+  const float r0 = rcp(s0), r1 = rcp(s1);
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    w0[s] *= r0;
+    w1[s] *= r1;
+  }
+  return WANT_VALUE ? (x1 - x0) + (lg2(s1) - lg2(s0)) : 0.0f;
+}
+
+struct AdjIo {
+  const float* llr;       // channel LLRs, [d0|d1|d2] per block
+  const float* sys_i;     // interleaved systematic LLRs (work layout)
+  const float* apr;       // the a-priori this SISO read in the forward pass (work layout)
+  const float* ge;        // d loss / d (scaled extrinsic of this SISO), work layout, natural order
+  const uint16_t* perm;   // lower SISO: position i's extrinsic is e2[perm[i]]
+  const float* seeds;     // [launch window][16]: the seeds this SISO used
+  float* own_sa;          // [work]: d loss / d(Ls+La) of the window's own steps (SISO order)
+  float* own_par;         // [work]: d loss / d Lp
+  float* guard_g;         // [launch window][4][guard]: alpha warm-up sa, par; beta warm-up sa, par
+  float* tail_g;          // [launch window][8]: d/d ts[0..2], d/d tp[0..2] (tail-started windows)
+  float* scale_part;      // [launch window]: sum of ge * x over the window
+  float4* ckpt;           // [launch window][2 * ckpt_slots]: alpha then beta checkpoints
+  int ckpt_slots;         // checkpoints of each kind per window
+  float scale;
+  int guard;
+};
+
+__device__ __forceinline__ void load8(const float* p, float (&m)[8]) {
+  const float4 x = ld4(p), y = ld4(p + 4);
+  m[0] = x.x; m[1] = x.y; m[2] = x.z; m[3] = x.w; m[4] = y.x; m[5] = y.y; m[6] = y.z; m[7] = y.w;
+}
+
+// d loss / d e of 4 consecutive positions of this SISO
+__device__ __forceinline__ void load_ge(const AdjIo& io, const DevCb& cb, bool lower, int q,
+                                        float (&ge)[4]) {
+  if (!lower) {
+    const float4 v = ld4(io.ge + cb.work + q);
+    ge[0] = v.x; ge[1] = v.y; ge[2] = v.z; ge[3] = v.w;
+  } else {
+    const uint2 iv = __ldg(reinterpret_cast<const uint2*>(io.perm + cb.tab + q));
+    ge[0] = __ldg(io.ge + cb.work + (iv.x & 0xffffu));
+    ge[1] = __ldg(io.ge + cb.work + (iv.x >> 16));
+    ge[2] = __ldg(io.ge + cb.work + (iv.y & 0xffffu));
+    ge[3] = __ldg(io.ge + cb.work + (iv.y >> 16));
+  }
+}
+
+template <bool LOWER>
+__global__ void __launch_bounds__(kAdjThreads) siso_adjoint_kernel(const DevCb* __restrict__ cbs,
+                                                                  const int32_t* __restrict__ win_cb,
+                                                                  int n_win, AdjIo io) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_win) return;
+  const DevCb cb = cbs[win_cb[g]];
+  const int w = g - cb.win0;
+  const int K = cb.k, W = cb.window, G = io.guard;
+  const int lo = w * W, hi = min(lo + W, K);
+  int a_lo = lo - G, b_hi = hi + G;
+  const bool start = a_lo <= 0, tail = b_hi >= K;
+  if (start) a_lo = 0;
+  if (tail) b_hi = K;
+  const float* d0 = io.llr + cb.llr;
+  const float* sys = LOWER ? io.sys_i + cb.work : d0;
+  const float* par = d0 + (LOWER ? 2 : 1) * (K + 4);
+  const float* apr = io.apr + cb.work;
+  const CkptGlobal cka{io.ckpt + static_cast<int64_t>(4) * io.ckpt_slots * g};
+  const CkptGlobal ckb{io.ckpt + static_cast<int64_t>(4) * io.ckpt_slots * g + 2 * io.ckpt_slots};
+  float sa[4], a[4], b[4];
+
+  // ---- A: alpha checkpoints at a_lo + 4m ----
+  float al[8];
+  if (start) alpha_start(al); else load8(io.seeds + 16 * g, al);
+  for (int q = a_lo; q < hi; q += 4) {
+    cka.store((q - a_lo) >> 2, al);
+    scale4(load_raw4(sys, apr, par, q), sa, a, b);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) alpha_step(al, a[t], b[t]);
+  }
+
+  // ---- B: backward in time ----
+  float be[8];
+  if (tail) {
+    float ts[3], tp[3];
+    tail_llrs(LOWER, d0, K, ts, tp);
+    tail_beta(be, ts, tp);
+  } else {
+    load8(io.seeds + 16 * g + 8, be);
+  }
+  for (int P = b_hi; P > hi; P -= 4) {  // beta warm-up: checkpoints at lo + 4m
+    ckb.store((P - lo) >> 2, be);
+    scale4(load_raw4(sys, apr, par, P - 4), sa, a, b);
+#pragma unroll
+    for (int t = 3; t >= 0; --t) beta_step(be, a[t], b[t]);
+  }
+  float ab[8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) ab[s] = 0.0f;
+  float spart = 0.0f;
+  const float xs = kLn2 * io.scale;  // d e / d(base-2 extrinsic)
+  for (int P = hi; P > lo; P -= 4) {  // the window's own steps
+    ckb.store((P - lo) >> 2, be);
+    const int q = P - 4;
+    scale4(load_raw4(sys, apr, par, q), sa, a, b);
+    float ge[4];
+    load_ge(io, cb, LOWER, q, ge);
+    float Al[4][8];
+    cka.load((q - a_lo) >> 2, Al[0]);
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+#pragma unroll
+      for (int s = 0; s < 8; ++s) Al[t + 1][s] = Al[t][s];
+      alpha_step(Al[t + 1], a[t], b[t]);
+    }
+    float gsa[4], gpar[4];
+#pragma unroll
+    for (int t = 3; t >= 0; --t) {
+      float w0[8], w1[8];
+      const float d2 = ext_weights<true>(Al[t], be, b[t], w0, w1);
+      spart += ge[t] * (kLn2 * d2);
+      const float G2 = xs * ge[t];
+      float nab[8], ga = 0.0f, gb = 0.0f;
+#pragma unroll
+      for (int s = 0; s < 8; ++s) {
+        nab[s] = G2 * (w1[s] - w0[s]);
+        gb += G2 * ((parity(s, 1) ? w1[s] : -w1[s]) - (parity(s, 0) ? w0[s] : -w0[s]));
+      }
+      alpha_adjoint(Al[t], a[t], b[t], ab, nab, ga, gb);
+#pragma unroll
+      for (int s = 0; s < 8; ++s) ab[s] = nab[s];
+      beta_step(be, a[t], b[t]);
+      gsa[t] = kHalfLog2e * ga;
+      gpar[t] = kHalfLog2e * gb;
+    }
+    *reinterpret_cast<float4*>(io.own_sa + cb.work + q) = make_float4(gsa[0], gsa[1], gsa[2], gsa[3]);
+    *reinterpret_cast<float4*>(io.own_par + cb.work + q) = make_float4(gpar[0], gpar[1], gpar[2], gpar[3]);
+  }
+  float* ag = io.guard_g + static_cast<int64_t>(4 * g) * G;
+  for (int P = lo; P > a_lo; P -= 4) {  // alpha warm-up steps
+    const int q = P - 4;
+    scale4(load_raw4(sys, apr, par, q), sa, a, b);
+    float Al[4][8];
+    cka.load((q - a_lo) >> 2, Al[0]);
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+#pragma unroll
+      for (int s = 0; s < 8; ++s) Al[t + 1][s] = Al[t][s];
+      alpha_step(Al[t + 1], a[t], b[t]);
+    }
+    float gsa[4], gpar[4];
+#pragma unroll
+    for (int t = 3; t >= 0; --t) {
+      float nab[8], ga = 0.0f, gb = 0.0f;
+#pragma unroll
+      for (int s = 0; s < 8; ++s) nab[s] = 0.0f;
+      alpha_adjoint(Al[t], a[t], b[t], ab, nab, ga, gb);
+#pragma unroll
+      for (int s = 0; s < 8; ++s) ab[s] = nab[s];
+      gsa[t] = kHalfLog2e * ga;
+      gpar[t] = kHalfLog2e * gb;
+    }
+    const int j = q - (lo - G);  // index within the G warm-up steps before lo
+    *reinterpret_cast<float4*>(ag + j) = make_float4(gsa[0], gsa[1], gsa[2], gsa[3]);
+    *reinterpret_cast<float4*>(ag + G + j) = make_float4(gpar[0], gpar[1], gpar[2], gpar[3]);
+  }
+  io.scale_part[g] = spart;
+
+  // ---- C: forward in time ----
+  float bb[8];
+#pragma unroll
+  for (int s = 0; s < 8; ++s) bb[s] = 0.0f;
+  cka.load((lo - a_lo) >> 2, al);
+  float* bg = ag + 2 * G;
+  for (int P = lo; P < b_hi; P += 4) {
+    scale4(load_raw4(sys, apr, par, P), sa, a, b);
+    float Bt[4][8];  // Bt[t] = beta at P + t + 1
+    ckb.load((P + 4 - lo) >> 2, Bt[3]);
+#pragma unroll
+    for (int t = 3; t > 0; --t) {
+#pragma unroll
+      for (int s = 0; s < 8; ++s) Bt[t - 1][s] = Bt[t][s];
+      beta_step(Bt[t - 1], a[t], b[t]);
+    }
+    const bool own = P < hi;
+    float ge[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (own) load_ge(io, cb, LOWER, P, ge);
+    float gsa[4], gpar[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      float nbb[8], ga = 0.0f, gb = 0.0f;
+#pragma unroll
+      for (int s = 0; s < 8; ++s) nbb[s] = 0.0f;
+      beta_adjoint(Bt[t], a[t], b[t], bb, nbb, ga, gb);
+      if (own) {
+        float w0[8], w1[8];
+        ext_weights<false>(al, Bt[t], b[t], w0, w1);
+        const float G2 = xs * ge[t];
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+          nbb[next_state(s, 0)] -= G2 * w0[s];
+          nbb[next_state(s, 1)] += G2 * w1[s];
+        }
+        alpha_step(al, a[t], b[t]);
+      }
+#pragma unroll
+      for (int s = 0; s < 8; ++s) bb[s] = nbb[s];
+      gsa[t] = kHalfLog2e * ga;
+      gpar[t] = kHalfLog2e * gb;
+    }
+    if (own) {
+      float4* ps = reinterpret_cast<float4*>(io.own_sa + cb.work + P);
+      float4* pp = reinterpret_cast<float4*>(io.own_par + cb.work + P);
+      const float4 s4 = *ps, p4 = *pp;
+      *ps = make_float4(s4.x + gsa[0], s4.y + gsa[1], s4.z + gsa[2], s4.w + gsa[3]);
+      *pp = make_float4(p4.x + gpar[0], p4.y + gpar[1], p4.z + gpar[2], p4.w + gpar[3]);
+    } else {
+      const int j = P - hi;
+      *reinterpret_cast<float4*>(bg + j) = make_float4(gsa[0], gsa[1], gsa[2], gsa[3]);
+      *reinterpret_cast<float4*>(bg + G + j) = make_float4(gpar[0], gpar[1], gpar[2], gpar[3]);
+    }
+  }
+  if (tail) {  // beta at K = the termination metrics (tail_beta): d/d tail LLRs
+    float gt[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int s0 = 0; s0 < 8; ++s0) {
+      int s = s0;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const int u = ((s >> 1) & 1) ^ ((s >> 2) & 1);
+        const int p = parity(s, u);
+        gt[i] += u ? bb[s0] : -bb[s0];
+        gt[3 + i] += p ? bb[s0] : -bb[s0];
+        s = next_state(s, u);
+      }
+    }
+    float* o = io.tail_g + 8 * g;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) o[i] = kHalfLog2e * gt[i];
+  }
+}
+
+struct CombineIo {
+  const DevCb* cbs;
+  const int64_t* start;   // first work position of each block
+  int n_cb;
+  int64_t total;
+  int guard;
+  const float* own_sa;
+  const float* own_par;
+  const float* guard_g;
+  const float* tail_g;
+  const uint16_t* perm;
+  const float* grad_post;  // posterior layout
+  float* grad_llr;         // LLR layout
+  float* ge_out;           // upper: d/d e2 of the previous iteration; lower: d/d e1 (natural)
+};
+
+// One thread per position of the SISO's order: own + neighbours' warm-up gradients, then
+// d0/d1/d2 and the adjoint of the a-priori (the other SISO's scaled extrinsic).
+template <bool LOWER, bool LAST>
+__global__ void adj_combine_kernel(CombineIo c) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= c.total) return;
+  int lo_c = 0, hi_c = c.n_cb - 1;
+  while (lo_c < hi_c) {
+    const int mid = (lo_c + hi_c + 1) >> 1;
+    if (c.start[mid] <= i) lo_c = mid; else hi_c = mid - 1;
+  }
+  const DevCb cb = c.cbs[lo_c];
+  const int p = static_cast<int>(i - c.start[lo_c]);
+  const int W = cb.window, G = c.guard, K = cb.k;
+  const int w = p / W, lo = w * W;
+  float sa = c.own_sa[cb.work + p], par = c.own_par[cb.work + p];
+  if (w + 1 < cb.nwin && p >= lo + W - G) {  // alpha warm-up of window w+1
+    const float* ag = c.guard_g + static_cast<int64_t>(4 * (cb.win0 + w + 1)) * G;
+    const int j = p - (lo + W - G);
+    sa += ag[j];
+    par += ag[G + j];
+  }
+  if (w > 0 && p < lo + G) {  // beta warm-up of window w-1
+    const float* bg = c.guard_g + static_cast<int64_t>(4 * (cb.win0 + w - 1)) * G + 2 * G;
+    const int j = p - lo;
+    sa += bg[j];
+    par += bg[G + j];
+  }
+  float* g0 = c.grad_llr + cb.llr;
+  float* g1 = g0 + (K + 4);
+  float* g2 = g1 + (K + 4);
+  if (!LOWER) {
+    g0[p] += sa;
+    g1[p] += par;
+    c.ge_out[cb.work + p] = sa;
+  } else {
+    const int q = c.perm[cb.tab + p];
+    g0[q] += sa;
+    g2[p] += par;
+    c.ge_out[cb.work + q] = sa + (LAST ? c.grad_post[cb.out + q] : 0.0f);
+  }
+  if (p == 0) {  // tail LLRs, summed over the tail-started windows in window order
+    float gt[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    for (int v = 0; v < cb.nwin; ++v) {
+      if (min((v + 1) * W, K) + G < K) continue;
+      const float* t = c.tail_g + 8 * (cb.win0 + v);
+      for (int k = 0; k < 6; ++k) gt[k] += t[k];
+    }
+    if (!LOWER) {  // ts = {d0[K], d0[K+2], 0}, tp = {d1[K], d0[K+1], d1[K+2]}
+      g0[K] += gt[0];
+      g0[K + 2] += gt[1];
+      g1[K] += gt[3];
+      g0[K + 1] += gt[4];
+      g1[K + 2] += gt[5];
+    } else {  // ts = {d1[K+3], d2[K], d2[K+2]}, tp = {d2[K+1], d0[K+3], d2[K+3]}
+      g1[K + 3] += gt[0];
+      g2[K] += gt[1];
+      g2[K + 2] += gt[2];
+      g2[K + 1] += gt[3];
+      g0[K + 3] += gt[4];
+      g2[K + 3] += gt[5];
+    }
+  }
+}
+
+// grad_llr: d0 gets d loss / d posterior (posterior = Ls + e1 + e2); ge2 = d loss / d e2 of the
+// last iteration (work layout).  grad_llr was zeroed before.
+__global__ void adj_init_kernel(const DevCb* __restrict__ cbs, const int64_t* __restrict__ start,
+                                int n_cb, int64_t total, const float* __restrict__ grad_post,
+                                float* __restrict__ grad_llr, float* __restrict__ ge2) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  int lo = 0, hi = n_cb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (start[mid] <= i) lo = mid; else hi = mid - 1;
+  }
+  const DevCb cb = cbs[lo];
+  const int64_t p = i - start[lo];
+  const float gp = grad_post[cb.out + p];
+  grad_llr[cb.llr + p] = gp;
+  ge2[cb.work + p] = gp;
+}
+
+// grad_scales[j] = sum over windows of part[j][window], in a fixed order (one block per j).
+__global__ void adj_scale_reduce_kernel(const float* __restrict__ part, int n_win,
+                                        float* __restrict__ grad_scales) {
+  __shared__ double acc[256];
+  const int j = blockIdx.x;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n_win; i += blockDim.x) s += part[static_cast<int64_t>(j) * n_win + i];
+  acc[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) acc[threadIdx.x] += acc[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) grad_scales[j] = static_cast<float>(acc[0]);
+}
+
+template <class T>
+T* reserve(DeviceBuffer& b, size_t count) {
+  b.reserve(count * sizeof(T));
+  return static_cast<T*>(b.ptr);
+}
+
+}  // namespace
+
+Adjoint::~Adjoint() {
+  for (DeviceBuffer* b : {&d_cbs_, &d_wincb_, &d_start_, &d_sysi_, &d_tape_, &d_seeds_, &d_ckpt_,
+                          &d_own_, &d_guard_, &d_tail_, &d_part_, &d_ge2_, &d_ga1_})
+    b->release();
+}
+
+uint64_t Adjoint::forward(const AdjointRequest& rq) {
+  std::lock_guard<std::mutex> lock(mu_);
+  ok(cudaSetDevice(dec_.device()), "cudaSetDevice");
+  cudaStream_t st = static_cast<cudaStream_t>(rq.stream);
+  have_tape_ = false;
+  const size_t n = rq.n_cb;
+  if (n == 0) throw InvalidArgument("no code blocks");
+  if (rq.iterations == 0 || rq.iterations > 64) throw InvalidArgument("iterations must be 1..64");
+  if (reinterpret_cast<uintptr_t>(rq.llr) % 16 != 0)
+    throw InvalidArgument("the LLR buffer must be 16-byte aligned");
+  const int guard = rq.guard < 0 ? kAdjGuard : rq.guard;
+  const int window_req = rq.window > 0 ? rq.window : kAdjWindow;
+  if (guard % kGroup != 0) throw InvalidArgument("guard must be a multiple of 8");
+  if (window_req % kGroup != 0) throw InvalidArgument("window must be a multiple of 8");
+
+  std::vector<DevCb> cbs_(n);
+  std::vector<int64_t> start(n);
+  std::vector<int32_t> wincb;
+  int64_t work = 0;
+  int max_window = 0;
+  for (size_t i = 0; i < n; ++i) {
+    const int32_t k = rq.cbs[i].k;
+    DevCb& d = cbs_[i];
+    d.tab = dec_.table_offset(k);
+    if (rq.cbs[i].filler < 0 || rq.cbs[i].filler >= k) throw InvalidArgument("invalid filler count");
+    if (rq.cbs[i].llr_offset < 0 || rq.cbs[i].llr_offset % 4 != 0 ||
+        static_cast<size_t>(rq.cbs[i].llr_offset) + 3 * static_cast<size_t>(k + 4) > rq.llr_len)
+      throw InvalidArgument("invalid LLR offset (must be a multiple of 4 and in range)");
+    if (rq.cbs[i].out_offset < 0 ||
+        static_cast<size_t>(rq.cbs[i].out_offset) + static_cast<size_t>(k) > rq.post_len)
+      throw InvalidArgument("invalid posterior offset");
+    d.k = k;
+    d.filler = rq.cbs[i].filler;
+    d.window = std::min<int32_t>(window_req, k);
+    if (guard > d.window && d.window < k) throw InvalidArgument("guard must not exceed the window");
+    d.nwin = (k + d.window - 1) / d.window;
+    d.win0 = static_cast<int32_t>(wincb.size());
+    d.llr = rq.cbs[i].llr_offset;
+    d.work = work;
+    d.out = rq.cbs[i].out_offset;
+    start[i] = work;
+    work += k;
+    max_window = std::max(max_window, d.window);
+    for (int w = 0; w < d.nwin; ++w) wincb.push_back(static_cast<int32_t>(i));
+  }
+  const int n_win = static_cast<int>(wincb.size());
+  const uint32_t I = rq.iterations;
+  n_cb_ = n;
+  llr_len_ = rq.llr_len;
+  post_len_ = rq.post_len;
+  work_ = work;
+  n_win_ = n_win;
+  guard_ = guard;
+  iterations_ = I;
+  llr_ = rq.llr;
+  scales_.assign(2 * I, 1.0f);
+  if (rq.scales) std::copy(rq.scales, rq.scales + 2 * I, scales_.begin());
+  ckpt_fwd_ = max_window / kSub;
+  ckpt_bwd_ = (max_window + guard) / 4 + 1;
+
+  DevCb* dcbs = reserve<DevCb>(d_cbs_, n);
+  int32_t* dwin = reserve<int32_t>(d_wincb_, n_win);
+  int64_t* dstart = reserve<int64_t>(d_start_, n);
+  float* sysi = reserve<float>(d_sysi_, work);
+  float* tape = reserve<float>(d_tape_, static_cast<size_t>(2 * I + 1) * work);
+  const size_t slab = static_cast<size_t>(n_win) * 16;
+  float* seeds = reserve<float>(d_seeds_, (2 * I + 2) * slab);
+  float4* ckpt = reserve<float4>(d_ckpt_, static_cast<size_t>(n_win) * 2 * ckpt_fwd_);
+  ok(cudaMemcpyAsync(dcbs, cbs_.data(), n * sizeof(DevCb), cudaMemcpyHostToDevice, st), "copy descriptors");
+  ok(cudaMemcpyAsync(dwin, wincb.data(), n_win * sizeof(int32_t), cudaMemcpyHostToDevice, st), "copy descriptors");
+  ok(cudaMemcpyAsync(dstart, start.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, st), "copy descriptors");
+  ok(cudaMemsetAsync(seeds, 0, 2 * slab * sizeof(float), st), "zero seeds");
+  const uint16_t* dperm = dec_.perm_table();
+  const uint16_t* dinv = dec_.inv_table();
+  // sys_i and tape slot 0 (the first a-priori, zero)
+  setup_kernel<<<static_cast<unsigned>((work + 255) / 256), 256, 0, st>>>(
+      dcbs, dstart, static_cast<int>(n), work, rq.llr, dperm, sysi, tape);
+  ok(cudaGetLastError(), "setup launch");
+  launches_ += 1;
+  const int blocks = (n_win + kThreads - 1) / kThreads;
+  for (uint32_t j = 0; j < 2 * I; ++j) {
+    const bool lower = j & 1;
+    SisoIo io{rq.llr, sysi, tape + j * work, tape + (j + 1) * work,
+              (j + 1 == 2 * I) ? rq.posterior : nullptr, dperm, dinv, seeds + j * slab,
+              seeds + (j + 2) * slab, scales_[j], guard};
+    if (!lower)
+      siso_plain_kernel<kSub, 0, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
+    else if (j + 1 < 2 * I)
+      siso_plain_kernel<kSub, 1, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
+    else
+      siso_plain_kernel<kSub, 2, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
+    ok(cudaGetLastError(), "SISO launch");
+    launches_ += 1;
+  }
+  have_tape_ = true;
+  return ++tape_id_;
+}
+
+void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr,
+                       float* grad_scales, void* stream) {
+  std::lock_guard<std::mutex> lock(mu_);
+  if (!have_tape_ || tape_id != tape_id_)
+    throw InvalidArgument("the tape of this forward pass was replaced by a later forward pass");
+  ok(cudaSetDevice(dec_.device()), "cudaSetDevice");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t work = work_;
+  const int n_win = n_win_, G = guard_;
+  const uint32_t I = iterations_;
+  const size_t slab = static_cast<size_t>(n_win) * 16;
+  float* own = reserve<float>(d_own_, 2 * static_cast<size_t>(work));
+  float* guard_g = reserve<float>(d_guard_, static_cast<size_t>(n_win) * 4 * std::max(G, 4));
+  float* tail_g = reserve<float>(d_tail_, static_cast<size_t>(n_win) * 8);
+  float* part = reserve<float>(d_part_, static_cast<size_t>(2 * I) * n_win);
+  float* ge2 = reserve<float>(d_ge2_, work);
+  float* ga1 = reserve<float>(d_ga1_, work);
+  float4* ckpt = reserve<float4>(d_ckpt_, static_cast<size_t>(n_win) * 4 * ckpt_bwd_);
+  const DevCb* dcbs = static_cast<const DevCb*>(d_cbs_.ptr);
+  const int32_t* dwin = static_cast<const int32_t*>(d_wincb_.ptr);
+  const int64_t* dstart = static_cast<const int64_t*>(d_start_.ptr);
+  const float* sysi = static_cast<const float*>(d_sysi_.ptr);
+  const float* tape = static_cast<const float*>(d_tape_.ptr);
+  const float* seeds = static_cast<const float*>(d_seeds_.ptr);
+  const uint16_t* dperm = dec_.perm_table();
+  const int n = static_cast<int>(n_cb_);
+  const unsigned pos_blocks = static_cast<unsigned>((work + 255) / 256);
+
+  ok(cudaMemsetAsync(grad_llr, 0, llr_len_ * sizeof(float), st), "zero grad_llr");
+  adj_init_kernel<<<pos_blocks, 256, 0, st>>>(dcbs, dstart, n, work, grad_post, grad_llr, ge2);
+  ok(cudaGetLastError(), "adjoint init launch");
+  launches_ += 1;
+  const int blocks = (n_win + kAdjThreads - 1) / kAdjThreads;
+  for (int j = static_cast<int>(2 * I) - 1; j >= 0; --j) {
+    const bool lower = j & 1;
+    const bool last = j + 2 >= static_cast<int>(2 * I);  // a SISO of the last iteration
+    AdjIo io{llr_, sysi, tape + j * work, lower ? ge2 : ga1, dperm, seeds + j * slab, own,
+             own + work, guard_g, tail_g, part + static_cast<int64_t>(j) * n_win, ckpt, ckpt_bwd_,
+             scales_[j], G};
+    if (lower)
+      siso_adjoint_kernel<true><<<blocks, kAdjThreads, 0, st>>>(dcbs, dwin, n_win, io);
+    else
+      siso_adjoint_kernel<false><<<blocks, kAdjThreads, 0, st>>>(dcbs, dwin, n_win, io);
+    ok(cudaGetLastError(), "SISO adjoint launch");
+    CombineIo c{dcbs, dstart, n, work, G, own, own + work, guard_g, tail_g, dperm, grad_post,
+                grad_llr, lower ? ga1 : ge2};
+    if (lower && last)
+      adj_combine_kernel<true, true><<<pos_blocks, 256, 0, st>>>(c);
+    else if (lower)
+      adj_combine_kernel<true, false><<<pos_blocks, 256, 0, st>>>(c);
+    else
+      adj_combine_kernel<false, false><<<pos_blocks, 256, 0, st>>>(c);
+    ok(cudaGetLastError(), "adjoint combine launch");
+    launches_ += 2;
+  }
+  adj_scale_reduce_kernel<<<2 * I, 256, 0, st>>>(part, n_win, grad_scales);
+  ok(cudaGetLastError(), "scale reduce launch");
+  launches_ += 1;
+}
+
+}  // namespace tcb

@@ -6,6 +6,7 @@
 #include <string>
 
 #include "../../include/turbo_b200.h"
+#include "adjoint.hpp"
 #include "decoder.hpp"
 #include "lte_codec.hpp"
 
@@ -60,6 +61,11 @@ tcb::CrcKind crc_kind(int kind) {
 struct tc_decoder {
   explicit tc_decoder(int device) : impl(device) {}
   tcb::Decoder impl;
+};
+
+struct tc_adjoint {
+  explicit tc_adjoint(tcb::Decoder& d) : impl(d) {}
+  tcb::Adjoint impl;
 };
 
 extern "C" {
@@ -437,6 +443,56 @@ int tc_decoder_timing(tc_decoder* dec, tc_timing* out, int reset) {
     out->siso_launches = t.siso_launches;
     out->siso_ms = t.siso_ms;
     out->trellis_steps = t.trellis_steps;
+  });
+}
+
+int tc_adjoint_create(tc_decoder* dec, tc_adjoint** out) {
+  return guarded([&] {
+    need(dec != nullptr && out != nullptr, "null pointer");
+    *out = nullptr;
+    *out = new tc_adjoint(dec->impl);
+  });
+}
+
+int tc_adjoint_destroy(tc_adjoint* adj) {
+  return guarded([&] { delete adj; });
+}
+
+int tc_adjoint_forward(tc_adjoint* adj, size_t n_cb, const tc_code_block* cbs, size_t llr_len,
+                       const float* llr, size_t post_len, float* posterior, uint32_t iterations,
+                       const float* scales, int32_t window, int32_t guard, void* stream,
+                       uint64_t* tape) {
+  return guarded([&] {
+    need(adj != nullptr && tape != nullptr, "null pointer");
+    need(n_cb > 0 && cbs && llr && posterior, "null pointer or no code blocks");
+    tcb::AdjointRequest rq;
+    rq.n_cb = n_cb;
+    rq.cbs = reinterpret_cast<const tcb::CodeBlockDesc*>(cbs);
+    rq.llr_len = llr_len;
+    rq.llr = llr;
+    rq.post_len = post_len;
+    rq.posterior = posterior;
+    rq.iterations = iterations;
+    rq.scales = scales;
+    rq.window = window;
+    rq.guard = guard;
+    rq.stream = stream;
+    *tape = adj->impl.forward(rq);
+  });
+}
+
+int tc_adjoint_backward(tc_adjoint* adj, uint64_t tape, const float* grad_posterior,
+                        float* grad_llr, float* grad_scales, void* stream) {
+  return guarded([&] {
+    need(adj && grad_posterior && grad_llr && grad_scales, "null pointer");
+    adj->impl.backward(tape, grad_posterior, grad_llr, grad_scales, stream);
+  });
+}
+
+int tc_adjoint_launches(tc_adjoint* adj, uint64_t* launches) {
+  return guarded([&] {
+    need(adj && launches, "null pointer");
+    *launches = adj->impl.launches();
   });
 }
 

@@ -242,6 +242,12 @@ Timing Decoder::timing(bool reset) {
   return t;
 }
 
+int32_t Decoder::table_offset(int32_t k) const {
+  const int qi = qpp_index(k);
+  if (qi < 0) throw OutOfRange("unsupported QPP block size");
+  return tab_offset_[qi];
+}
+
 int Decoder::pick_window(int32_t k, int32_t requested) const {
   if (requested > 0) return std::min<int32_t>(requested, k);
   return std::min<int32_t>(kDefaultWindow, k);

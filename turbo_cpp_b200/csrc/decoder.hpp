@@ -153,6 +153,12 @@ class Decoder {
   void decode_transport_blocks(const TbRequest& q);
   int sm_count() const { return sm_count_; }
 
+  // QPP tables on the device (uint16 per position; all 188 sizes back to back) and the offset
+  // of block size k's table in them (throws OutOfRange for a size outside the table)
+  const uint16_t* perm_table() const { return static_cast<const uint16_t*>(d_perm_.ptr); }
+  const uint16_t* inv_table() const { return static_cast<const uint16_t*>(d_inv_.ptr); }
+  int32_t table_offset(int32_t k) const;
+
  private:
   int pick_window(int32_t k, int32_t requested) const;
   void decode_persistent(const DecodeRequest& rq);
