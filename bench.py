@@ -48,7 +48,7 @@ MUFU_PER_SM_CLK = 16  # B200 SFU lanes per SM per clock (4 per SM sub-partition)
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--n-cb", type=int, default=4096)
@@ -121,6 +121,9 @@ class ClockSampler:
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
                  "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            # nvidia-smi takes a few hundred ms to start: wait for its first sample (taken
+            # before the timed region, so dropped) before the caller starts timing
+            self.proc.stdout.readline()
         except OSError:
             self.proc = None
         return self
@@ -276,43 +279,136 @@ def config3_figure(tc, dev, iters):
     return out
 
 
+TRAINED_SCALES = os.path.join(ROOT, "turbo_cpp_b200", "data", "scales_k6144_0p6db_it6.json")
+
+
+def trained_scales(iters):
+    """The committed trained scales (6 iterations) extended to `iters` iterations by repeating
+    the last iteration's pair."""
+    with open(TRAINED_SCALES) as f:
+        sc = list(json.load(f)["scales"])
+    while len(sc) < 2 * iters:
+        sc += sc[-2:]
+    return sc[:2 * iters]
+
+
+def wilson(k, n, z=1.96):
+    if n == 0:
+        return (0.0, 1.0)
+    p = k / n
+    d = 1 + z * z / n
+    c = (p + z * z / (2 * n)) / d
+    h = z * np.sqrt(p * (1 - p) / n + z * z / (4 * n * n)) / d
+    return (float(c - h), float(c + h))
+
+
 def config5_figure(tc, dev, stream, iters):
     """20000 code blocks, K from all 188 sizes with P ~ K, CRC24B payloads, Eb/N0 ~ U[0, 2] dB,
-    early stop, one persistent launch: device-resident info Mbit/s (K-24 per block)."""
+    early stop, one launch: device-resident info Mbit/s (K-24 per block), plain unscaled
+    decoder and the trained scales; BLER at 0.6 dB on a second batch of the same K mix."""
     import torch
     from turbo_cpp_b200.workloads import config5_code_blocks
 
-    ks, llr, bits, eb = config5_code_blocks(20000, seed=55)
-    cbs, llr_len, post_len = tc.Decoder.layout(ks)
-    x = torch.from_numpy(llr).cuda()
-    post = torch.empty(post_len, dtype=torch.float32, device="cuda")
-    itd = torch.zeros(ks.size, dtype=torch.int32, device="cuda")
-    info = int(np.sum(ks - 24))
-    out = {}
-    for name, sched in (("persistent", tc.SCHEDULE_PERSISTENT), ("plain", tc.SCHEDULE_PLAIN)):
-        o = tc.DecodeOptions(iters, True, 0, -1, sched)
+    def run(ks, llr, bits, o, reps):
+        cbs, llr_len, post_len = tc.Decoder.layout(ks)
+        x = torch.from_numpy(llr).cuda()
+        post = torch.empty(post_len, dtype=torch.float32, device="cuda")
+        itd = torch.zeros(ks.size, dtype=torch.int32, device="cuda")
         dev.decode_device(cbs, ks.size, x.data_ptr(), llr_len, post.data_ptr(), post_len, 0,
                           itd.data_ptr(), options=o, stream=stream.cuda_stream)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(3):
+        for _ in range(reps):
             dev.decode_device(cbs, ks.size, x.data_ptr(), llr_len, post.data_ptr(), post_len, 0,
                               itd.data_ptr(), options=o, stream=stream.cuda_stream)
         e1.record(stream)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / 3
-        p = post.cpu().numpy()
-        errs = (p >= 0) != bits
+        errs = (post.cpu().numpy() >= 0) != bits
         starts = np.concatenate([[0], np.cumsum(ks)[:-1]])
-        blk = np.logical_or.reduceat(errs, starts)
+        return e0.elapsed_time(e1) / reps, np.logical_or.reduceat(errs, starts), itd
+
+    ks, llr, bits, eb = config5_code_blocks(20000, seed=55)
+    ks6, llr6, bits6, _ = config5_code_blocks(8000, seed=56, ebn0_range=(0.6, 0.6))
+    info = int(np.sum(ks - 24))
+    scales = trained_scales(iters)
+    out = {}
+    for name, sched, sc in (("persistent", tc.SCHEDULE_PERSISTENT, None),
+                            ("plain", tc.SCHEDULE_PLAIN, None),
+                            ("persistent_trained_scales", tc.SCHEDULE_PERSISTENT, scales)):
+        o = tc.DecodeOptions(iters, True, 0, -1, sched, scales=sc)
+        ms, blk, itd = run(ks, llr, bits, o, 3)
+        _, blk6, _ = run(ks6, llr6, bits6, o, 1)
         sel = (eb > 0.5) & (eb < 0.7)
+        k6 = int(blk6.sum())
         out[name] = {"value": info / ms / 1e3, "unit": "Mbit/s", "ms": ms,
                      "mean_iterations": float(itd.float().mean().item()),
-                     "bler": float(blk.mean()), "bler_0.5_0.7dB": float(blk[sel].mean())}
+                     "bler": float(blk.mean()), "bler_0.5_0.7dB": float(blk[sel].mean()),
+                     "bler_0.6dB": k6 / blk6.size, "bler_0.6dB_ci95": wilson(k6, blk6.size)}
+    out["trained_scales"] = [round(v, 4) for v in scales]
     out["workload"] = ("20000 code blocks, K over all 188 QPP sizes with P ~ K, K-24 payload + "
                        "CRC24B, Eb/N0 ~ U[0,2] dB per block, 8 max iterations, CRC24B early "
-                       "stop, device-resident LLRs")
+                       "stop, device-resident LLRs; bler_0.6dB: 8000 blocks of the same K mix at "
+                       "0.6 dB; trained scales: the committed 6-iteration scales, the last "
+                       "pair repeated for iterations 7 and 8")
     return out
+
+
+def config4_figure(tc, dev):
+    """Differentiation workload: 1024 blocks of K=6144 at 0.6 dB, 6 unrolled iterations, 12
+    scales, loss = mean BCE of the posterior; one training step = forward with tape + the
+    hand-written backward (torch autograd through the libtorch wrapper), inputs resident."""
+    import torch
+    import torch.nn.functional as F
+    from turbo_cpp_b200.autograd import DifferentiableDecoder
+
+    n, k = 1024, 6144
+    ks = [k] * n
+    bits, llr = tc.awgn_code_blocks(44, ks, 0.6)
+    dd = DifferentiableDecoder(ks, decoder=dev)
+    x = torch.from_numpy(llr).cuda()
+    b = torch.from_numpy(bits).cuda().float()
+    sc = torch.ones(12, device="cuda", requires_grad=True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+
+    def step(split=False):
+        if split:
+            ev[0].record()
+        post = dd(x, sc)
+        loss = F.binary_cross_entropy_with_logits(post, b)
+        if split:
+            ev[1].record()
+        loss.backward()
+        if split:
+            ev[2].record()
+        return loss
+
+    for _ in range(3):
+        step()
+    fwd = bwd = 0.0
+    for _ in range(3):
+        step(split=True)
+        torch.cuda.synchronize()
+        fwd += ev[0].elapsed_time(ev[1]) / 3
+        bwd += ev[1].elapsed_time(ev[2]) / 3
+    reps = 10
+    launches0 = dd.adjoint.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    with open(TRAINED_SCALES) as f:
+        tr = json.load(f)
+    return {"value": n * k / ms / 1e3, "unit": "info Mbit/s through forward + backward",
+            "ms_per_step": ms, "forward_ms": fwd, "backward_ms": bwd,
+            "library_launches_per_step": (dd.adjoint.launches() - launches0) // reps,
+            "trained_scales": [round(v, 4) for v in tr["scales"]],
+            "training": {k2: tr.get(k2) for k2 in ("command", "held_out", "wall_s")},
+            "gradient_check": "tests/test_gpu_adjoint.py: K=40 GPU gradients vs FP64 central "
+                              "finite differences (h=1e-4) and the FP64 adjoint, 1e-4 bar",
+            "workload": "1024 x K=6144, 0.6 dB, 6 iterations, window 64, guard 32, 12 scales"}
 
 
 def ber_bler(post, bits, n, k):
@@ -506,6 +602,7 @@ def main():
     if not args.no_configs:
         line["config3_chain"] = config3_figure(tc, dev, it)
         line["config5_mixed"] = config5_figure(tc, dev, stream, it)
+        line["config4_adjoint"] = config4_figure(tc, dev)
 
     # ---- plain per-block GPU path: one code block per call, as the reference API decodes ----
     per_block = []

@@ -51,7 +51,9 @@ def test_autograd_equals_c_abi(tc, decoder):
 def test_training_harness_runs(tc):
     from turbo_cpp_b200.train import train_scales
 
-    sc, hist = train_scales(steps=6, n_blocks=64, k=1024, ebn0_db=0.6, iterations=6, lr=0.05)
+    sc, hist, held = train_scales(steps=6, n_blocks=64, k=1024, ebn0_db=0.6, iterations=6,
+                                  lr=0.05)
     assert sc.shape == (12,) and np.all(np.isfinite(sc))
     assert len(hist) == 6 and all(np.isfinite(h["loss"]) for h in hist)
     assert not np.allclose(sc, 1.0)  # the scales moved
+    assert np.isfinite(held["initial"]["loss"]) and np.isfinite(held["trained"]["loss"])

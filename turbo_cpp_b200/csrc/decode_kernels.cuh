@@ -157,9 +157,7 @@ __device__ __forceinline__ void store_release(int* p, int v) {
 
 __global__ void __launch_bounds__(kPersistThreads, kPersistMinBlocks)
     persistent_kernel(const PersistArgs p) {
-  __shared__ uint32_t syn[kPersistThreads];
   const int lane = threadIdx.x & 31;
-  const int wbase = threadIdx.x & ~31;
   const int total = p.n_tasks * 2 * p.max_iterations;
   for (;;) {
     int item = 0;
@@ -200,7 +198,9 @@ __global__ void __launch_bounds__(kPersistThreads, kPersistMinBlocks)
         siso_window_rt<kSub, CkptGlobal, true>(cb, w, g, io, ck, half == 1, half == 1 && post_now);
       if (half == 1 && p.early_stop) {
         // CRC24B syndrome of the hard decisions (lte_turbo.cpp:792-804): each lane XORs
-        // x^(N-1-i) mod g over the set bits of its window, the block's first lane combines.
+        // x^(N-1-i) mod g over the set bits of its window; a block's windows sit in consecutive
+        // lanes, so its first lane takes the XOR of their parts from a warp-wide XOR prefix
+        // scan (no shared memory, which keeps the occupancy at the register limit).
         __threadfence();  // this lane's posterior stores, before the other lanes read them
         __syncwarp();
         uint32_t part = 0;
@@ -210,11 +210,17 @@ __global__ void __launch_bounds__(kPersistThreads, kPersistMinBlocks)
           for (int q = max(lo_p, cb.filler); q < hi_p; ++q)
             if (__ldcg(p.post + cb.out + q) >= 0.0f) part ^= p.xpow[n - 1 - (q - cb.filler)];
         }
-        syn[threadIdx.x] = part;
-        __syncwarp();
+        uint32_t pre = part;  // part[0] ^ ... ^ part[lane]
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t v = __shfl_up_sync(0xffffffffu, pre, o);
+          if (lane >= o) pre ^= v;
+        }
+        const int last = min(lane + max(cb.nwin, 1) - 1, 31);
+        const uint32_t upto_last = __shfl_sync(0xffffffffu, pre, last);
+        const uint32_t before = __shfl_sync(0xffffffffu, pre, lane > 0 ? lane - 1 : 0);
         if (active && w == 0) {
-          uint32_t x = 0;
-          for (int j = 0; j < cb.nwin; ++j) x ^= syn[wbase + lane + j];
+          const uint32_t x = upto_last ^ (lane > 0 ? before : 0u);
           p.iters[c] = static_cast<uint32_t>(it + 1);
           if (x == 0) p.done[c] = 1;
         }

@@ -39,8 +39,24 @@ def train_scales(steps: int = 200, n_blocks: int = 1024, k: int = 6144, ebn0_db:
     # moving by about lr around their optimum
     sched = torch.optim.lr_scheduler.LambdaLR(
         opt, lambda i: 0.1 + 0.45 * (1.0 + np.cos(np.pi * min(i, steps) / max(steps, 1))))
+    # cosine decay to lr/10: the batch-to-batch noise of the loss otherwise keeps the scales
+    # moving by about lr around their optimum
+    sched = torch.optim.lr_scheduler.LambdaLR(
+        opt, lambda i: 0.1 + 0.45 * (1.0 + np.cos(np.pi * min(i, steps) / max(steps, 1))))
     history = []
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    vbits, vllr = awgn_code_blocks(seed + 1000000, ks, ebn0_db)
+    vx = torch.from_numpy(vllr).to(dev)
+    vb = torch.from_numpy(vbits).to(dev, torch.float32)
+
+    def held_out(sc):
+        with torch.no_grad():
+            post = dd(vx, sc)
+            errs = ((post >= 0).float() != vb).float().view(n_blocks, k)
+            return dict(loss=float(F.binary_cross_entropy_with_logits(post, vb)),
+                        ber=float(errs.mean()), bler=float(errs.amax(1).mean()))
+
+    held = {"initial": held_out(scales.detach())}
     with ThreadPoolExecutor(1) as pool:
         fut = pool.submit(awgn_code_blocks, seed, ks, ebn0_db)
         for step in range(steps):
@@ -57,6 +73,7 @@ def train_scales(steps: int = 200, n_blocks: int = 1024, k: int = 6144, ebn0_db:
             ev[1].record()
             opt.step()
             sched.step()
+            sched.step()
             with torch.no_grad():
                 errs = ((post >= 0).float() != b).float().view(n_blocks, k)
             rec = dict(step=step, loss=float(loss.detach()), ber=float(errs.mean()),
@@ -65,7 +82,8 @@ def train_scales(steps: int = 200, n_blocks: int = 1024, k: int = 6144, ebn0_db:
             history.append(rec)
             if callback:
                 callback(rec)
-    return scales.detach().cpu().numpy().astype(np.float32), history
+    held["trained"] = held_out(scales.detach())
+    return scales.detach().cpu().numpy().astype(np.float32), history, held
 
 
 def main(argv=None) -> None:
@@ -90,15 +108,15 @@ def main(argv=None) -> None:
                   f"bler {r['bler']:.3f} step_ms {r['ms']:.2f} scales "
                   + " ".join(f"{v:.3f}" for v in r["scales"]), flush=True)
 
-    sc, hist = train_scales(a.steps, a.blocks, a.k, a.ebn0, a.iterations, a.lr, a.seed, a.window,
+    sc, hist, held = train_scales(a.steps, a.blocks, a.k, a.ebn0, a.iterations, a.lr, a.seed, a.window,
                             a.guard, callback=show)
     out = dict(scales=[float(v) for v in sc], steps=a.steps, blocks=a.blocks, k=a.k,
                ebn0_db=a.ebn0, iterations=a.iterations, lr=a.lr, seed=a.seed,
-               wall_s=time.time() - t0, history=hist)
+               wall_s=time.time() - t0, held_out=held, history=hist)
     if a.out:
         with open(a.out, "w") as f:
             json.dump(out, f)
-    print(json.dumps({key: out[key] for key in ("scales", "wall_s")}))
+    print(json.dumps({key: out[key] for key in ("scales", "wall_s", "held_out")}))
 
 
 if __name__ == "__main__":
