@@ -108,7 +108,13 @@ typedef struct {
   int64_t out_offset; /* float offset of the block's K posterior LLRs                     */
 } tc_code_block;
 
-enum { TC_MEM_HOST = 0, TC_MEM_DEVICE = 1 };
+/* HOST: synchronous, the call copies the LLRs in and the results out.  DEVICE: device pointers,
+ * ordered on opts->stream, returns once enqueued.  HOST_ASYNC (new): host pointers; the call
+ * enqueues copy-in, decode and copy-out on one of three internal device workspaces (used in
+ * turn, each with its own stream) and returns, so that one call's copies run while earlier
+ * calls decode; results are valid, and the input buffer may be reused, after tc_decoder_sync.
+ * Pinned host memory is needed for the copies to overlap. */
+enum { TC_MEM_HOST = 0, TC_MEM_DEVICE = 1, TC_MEM_HOST_ASYNC = 2 };
 /* PLAIN: one launch per SISO half-iteration over all blocks (host-driven iteration loop).
  * PERSISTENT: one launch for all iterations, warps pull (task, half-iteration) items from a
  * device queue, blocks stop individually on CRC24B.  AUTO: the schedule and window that
@@ -120,7 +126,7 @@ typedef struct {
   uint32_t early_stop;     /* stop a block once its hard decisions pass CRC24B            */
   int32_t window;          /* steps per window; 0 = default (128); >= K = full trellis    */
   int32_t guard;           /* warm-up steps on each side; < 0 = default (96); multiple of 8 */
-  uint32_t memory;         /* TC_MEM_HOST (synchronous, copies inside) or TC_MEM_DEVICE   */
+  uint32_t memory;         /* TC_MEM_HOST, TC_MEM_DEVICE or TC_MEM_HOST_ASYNC              */
   uint32_t schedule;       /* TC_SCHEDULE_PLAIN or TC_SCHEDULE_PERSISTENT                 */
   const float* scales;     /* host array, 2 per iteration (upper, lower); NULL = 1.0     */
   uint32_t graph;          /* TC_MEM_DEVICE only: capture this request's launch sequence in a

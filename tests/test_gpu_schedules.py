@@ -91,3 +91,34 @@ def test_persistent_wait_limit_reports_timeout(tc):
     post, _, _ = dec.decode(ks, llr, options=opts)  # the context and the decoder still work
     ref, _, _ = dec.decode(ks, llr, options=tc.DecodeOptions(2))
     assert np.all(np.isfinite(post)) and llr_close(post, ref, rtol=2e-3)[0] <= 2e-3
+
+
+@pytest.mark.parametrize("schedule", ["plain", "persistent"])
+def test_async_host_calls_match_synchronous_ones(tc, decoder, schedule):
+    """TC_MEM_HOST_ASYNC: five calls in a row on different inputs (pinned host buffers), then
+    one sync: every call's posterior, CRC flags and iteration counts equal a synchronous
+    host-memory call on the same input."""
+    import torch
+
+    sched = tc.SCHEDULE_PLAIN if schedule == "plain" else tc.SCHEDULE_PERSISTENT
+    rng = np.random.default_rng(23)
+    table = np.array([e.k for e in tc.qpp_interleaver_table()])
+    ks = rng.choice(table, 300)
+    cbs, llr_len, post_len = tc.Decoder.layout(ks)
+    o = tc.DecodeOptions(8, True, 0, -1, sched)
+    calls = []
+    for i in range(5):
+        llr, _ = awgn_blocks(tc, ks, 0.6 + 0.2 * i, seed=30 + i, crc24b=True)
+        x = torch.from_numpy(llr).pin_memory()
+        p = torch.full((post_len,), 7.0).pin_memory()
+        c = torch.zeros(len(ks), dtype=torch.uint8).pin_memory()
+        it = torch.zeros(len(ks), dtype=torch.int32).pin_memory()
+        decoder.decode_async(cbs, len(ks), x.data_ptr(), llr_len, p.data_ptr(), post_len,
+                             c.data_ptr(), it.data_ptr(), options=o)
+        calls.append((llr, x, p, c, it))
+    decoder.sync()
+    for llr, x, p, c, it in calls:
+        post, ok, used = decoder.decode(ks, llr, options=o)
+        assert np.array_equal(p.numpy(), post)
+        assert np.array_equal(c.numpy().astype(bool), np.asarray(ok, bool))
+        assert np.array_equal(it.numpy().astype(np.uint32), np.asarray(used, np.uint32))

@@ -32,7 +32,7 @@ __all__ = [
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libturbo_b200.so")
 
-MEM_HOST, MEM_DEVICE = 0, 1
+MEM_HOST, MEM_DEVICE, MEM_HOST_ASYNC = 0, 1, 2
 SCHEDULE_PLAIN, SCHEDULE_PERSISTENT, SCHEDULE_AUTO = 0, 1, 2
 
 
@@ -521,6 +521,17 @@ class Decoder:
     def sync(self) -> None:
         """Waits for enqueued work; raises DeviceTimeout if a device-side wait gave up."""
         _call("tc_decoder_sync", self._h)
+
+    def decode_async(self, cbs, n_cb: int, llr_ptr: int, llr_len: int, post_ptr: int,
+                     post_len: int, crc_ptr: int = 0, iters_ptr: int = 0,
+                     options: Optional[DecodeOptions] = None) -> None:
+        """TC_MEM_HOST_ASYNC: host pointers (pinned for overlap, e.g. torch pin_memory()
+        tensors); enqueues copy-in, decode and copy-out and returns.  Results are valid after
+        sync(); consecutive calls overlap one call's copies with earlier calls' decoding."""
+        o = options or DecodeOptions()
+        opt, _keep = self._opts(o, MEM_HOST_ASYNC)
+        _call("tc_decode", self._h, int(n_cb), C.addressof(cbs), int(llr_len), llr_ptr,
+              int(post_len), post_ptr, crc_ptr or None, iters_ptr or None, C.addressof(opt))
 
     def autotune(self, cbs, n_cb: int, llr_ptr: int, llr_len: int, post_ptr: int, post_len: int,
                  options: Optional[DecodeOptions] = None, stream: int = 0) -> dict:

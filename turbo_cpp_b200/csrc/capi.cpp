@@ -263,7 +263,8 @@ int tc_decode(tc_decoder* dec, size_t n_cb, const tc_code_block* cbs, size_t llr
     need(n_cb == 0 || (cbs && llr && posterior), "null pointer");
     tc_decode_options o;
     if (opts) o = *opts; else tc_decode_options_init(&o);
-    need(o.memory == TC_MEM_HOST || o.memory == TC_MEM_DEVICE, "unknown memory kind");
+    need(o.memory == TC_MEM_HOST || o.memory == TC_MEM_DEVICE || o.memory == TC_MEM_HOST_ASYNC,
+         "unknown memory kind");
     need(o.schedule == TC_SCHEDULE_PLAIN || o.schedule == TC_SCHEDULE_PERSISTENT ||
              o.schedule == TC_SCHEDULE_AUTO,
          "unknown schedule");
@@ -283,6 +284,7 @@ int tc_decode(tc_decoder* dec, size_t n_cb, const tc_code_block* cbs, size_t llr
     rq.window = o.window;
     rq.guard = o.guard;
     rq.device_memory = o.memory == TC_MEM_DEVICE;
+    rq.host_async = o.memory == TC_MEM_HOST_ASYNC;
     rq.persistent = o.schedule == TC_SCHEDULE_PERSISTENT;
     rq.auto_schedule = o.schedule == TC_SCHEDULE_AUTO;
     rq.graph = o.graph != 0;

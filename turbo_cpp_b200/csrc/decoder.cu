@@ -152,6 +152,7 @@ Decoder::~Decoder() {
     if (e.start) cudaEventDestroy(static_cast<cudaEvent_t>(e.start));
     if (e.stop) cudaEventDestroy(static_cast<cudaEvent_t>(e.stop));
   }
+  workers_.clear();  // each waits for its own work (cudaFree) and releases its buffers
   if (stream_) cudaStreamDestroy(static_cast<cudaStream_t>(stream_));
   for (DeviceBuffer* b : {&d_perm_, &d_inv_, &d_xpow_, &d_cbs_, &d_wincb_, &d_start_, &d_llr_,
                           &d_sysi_, &d_e1i_, &d_e2_, &d_post_, &d_seed_, &d_done_, &d_iters_,
@@ -193,6 +194,7 @@ void Decoder::sync() {
   check(cudaSetDevice(device_), "cudaSetDevice");
   if (last_event_)
     check(cudaEventSynchronize(static_cast<cudaEvent_t>(last_event_)), "cudaEventSynchronize");
+  for (auto& w : workers_) w->sync();  // asynchronous host-memory calls (and their timeouts)
   take_error();
 }
 
@@ -260,6 +262,10 @@ void Decoder::decode(const DecodeRequest& rq_in) {
     return;
   }
   std::lock_guard<std::mutex> lock(mu_);
+  if (rq.host_async) {
+    decode_host_async(rq);
+    return;
+  }
   if (rq.persistent)
     decode_persistent(rq);
   else
@@ -610,6 +616,54 @@ void Decoder::decode_plain(const DecodeRequest& rq) {
   }
   mark_done(st);
   if (!rq.device_memory) check(cudaStreamSynchronize(st), "sync");
+}
+
+// ------------------------------------------------------------------------------------------
+// Asynchronous host-memory calls
+// ------------------------------------------------------------------------------------------
+namespace {
+constexpr size_t kAsyncWorkers = 3;  // copy-in of call i+2 needs no wait for call i
+}  // namespace
+
+void Decoder::decode_host_async(const DecodeRequest& rq) {
+  if (rq.n_cb == 0) return;
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  while (workers_.size() < kAsyncWorkers) workers_.push_back(std::make_unique<Decoder>(device_));
+  Decoder& w = *workers_[next_worker_];
+  next_worker_ = (next_worker_ + 1) % workers_.size();
+  std::lock_guard<std::mutex> wl(w.mu_);
+  const uint64_t launches_before = w.timing_.launches;
+  cudaStream_t ws = static_cast<cudaStream_t>(w.stream_);
+  // this worker's previous call is ordered before on its own stream; a buffer that has to grow
+  // is freed with cudaFree, which waits for the device
+  float* dl = w.grow<float>(w.d_llr_, rq.llr_len);
+  float* dp = w.grow<float>(w.d_post_, rq.post_len);
+  uint8_t* dc = w.grow<uint8_t>(w.d_crc_, rq.n_cb);
+  uint32_t* di = w.grow<uint32_t>(w.d_iters_, rq.n_cb);
+  check(cudaMemcpyAsync(dl, rq.llr, rq.llr_len * sizeof(float), cudaMemcpyHostToDevice, ws),
+        "copy LLRs in");
+  // positions outside every block's range come back as 0, as in synchronous host calls
+  check(cudaMemsetAsync(dp, 0, rq.post_len * sizeof(float), ws), "zero posterior");
+  DecodeRequest r = rq;
+  r.llr = dl;
+  r.posterior = dp;
+  r.crc_ok = dc;
+  r.iterations_used = di;
+  r.device_memory = true;
+  r.host_async = false;
+  r.graph = false;
+  r.auto_schedule = false;
+  r.stream = ws;
+  if (r.persistent) w.decode_persistent(r); else w.decode_plain(r);
+  check(cudaMemcpyAsync(rq.posterior, dp, rq.post_len * sizeof(float), cudaMemcpyDeviceToHost, ws),
+        "copy posterior out");
+  if (rq.crc_ok)
+    check(cudaMemcpyAsync(rq.crc_ok, dc, rq.n_cb, cudaMemcpyDeviceToHost, ws), "copy crc out");
+  if (rq.iterations_used)
+    check(cudaMemcpyAsync(rq.iterations_used, di, rq.n_cb * sizeof(uint32_t),
+                          cudaMemcpyDeviceToHost, ws), "copy iters out");
+  w.mark_done(ws);
+  timing_.launches += w.timing_.launches - launches_before;
 }
 
 // ------------------------------------------------------------------------------------------

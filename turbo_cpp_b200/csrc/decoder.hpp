@@ -59,6 +59,7 @@ struct DecodeRequest {
   int window = 0;   // 0: default
   int guard = -1;   // <0: default
   bool device_memory = false;  // llr/posterior/crc_ok/iterations_used are device pointers
+  bool host_async = false;     // host pointers; enqueue copies + decode and return (see sync())
   bool smem_checkpoints = false;  // alpha checkpoints in shared memory instead of global scratch
   bool persistent = false;  // persistent warp-task schedule instead of per-half-iteration launches
   bool graph = false;       // device memory: capture the launch sequence once, replay it after
@@ -163,6 +164,12 @@ class Decoder {
   int pick_window(int32_t k, int32_t requested) const;
   void decode_persistent(const DecodeRequest& rq);
   void decode_plain(const DecodeRequest& rq);
+  // Asynchronous host-memory calls rotate over kAsyncWorkers worker decoders, each with its own
+  // device buffers and stream: a call enqueues copy-in, decode and copy-out on the next worker
+  // and returns, so that its copies run while the previous calls decode.  sync() waits for them.
+  void decode_host_async(const DecodeRequest& rq);
+  std::vector<std::unique_ptr<Decoder>> workers_;
+  size_t next_worker_ = 0;
   void decode_graph(const DecodeRequest& rq);
   // host -> device copy of launch descriptors; while capturing, from graph-owned pinned memory
   void upload(void* dst, const void* src, size_t bytes, void* stream);
