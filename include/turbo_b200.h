@@ -188,6 +188,16 @@ TC_API int tc_derate_match_llr_device(tc_decoder* dec, size_t n_cb, const tc_rm_
                                       size_t e_len, const float* e_llr, size_t llr_len,
                                       float* d012, void* stream);
 
+/* HARQ soft combining (new; the reference de-rate matches a single transmission,
+ * lte_turbo.cpp:280-325): the n_tx entries of tx are transmissions; those of one code block are
+ * consecutive and share llr_offset, K and filler (at most 8 per code block), each with its own
+ * rv, E and e_offset.  Each code block's [d0|d1|d2] becomes the sum, in the given order, of its
+ * transmissions' de-rate-matched LLRs -- bit-identical to tc_derate_match_llr per transmission
+ * followed by elementwise addition in that order.  Device pointers, ordered on `stream`. */
+TC_API int tc_derate_combine_llr_device(tc_decoder* dec, size_t n_tx, const tc_rm_block* tx,
+                                        size_t e_len, const float* e_llr, size_t llr_len,
+                                        float* d012, void* stream);
+
 /* Decodes many transport blocks at once (replaces decode_transport_block, lte_turbo.h:157-159,
  * lte_turbo.cpp:891-980, for any number of transport blocks per call): device de-rate matching,
  * batched turbo decoding with opts (schedule, early stop on CRC24B, iterations, ...), then per

@@ -78,3 +78,40 @@ def test_transport_block_chain_matches_reference(tc, decoder, oracle):
     # high Eb/N0 transport blocks decode to the transmitted bits
     good = [t for t in range(len(tbs)) if ebs[t] > 2.0]
     assert good and all(np.array_equal(bits[t], truth[t]) and tb_ok[t] for t in good)
+
+
+def test_harq_combining_matches_host_derate_sums(tc, decoder):
+    """tc_derate_combine_llr_device: 1-4 transmissions per code block (rv cycling 0, 2, 3, 1,
+    punctured and repeated E, fillers) give exactly the sum, in transmission order, of the host
+    de-rate matcher's output per transmission."""
+    import torch
+
+    rng = np.random.default_rng(41)
+    table = np.array([e.k for e in tc.qpp_interleaver_table()])
+    tx, host, e_parts = [], [], []
+    e_off = llr_off = 0
+    for b in range(24):
+        k = int(rng.choice(table))
+        f = int(rng.integers(0, 4)) * 8 if b % 3 == 0 else 0
+        f = min(f, k - 8)
+        acc = None
+        for t in range(int(rng.integers(1, 5))):
+            rv = (0, 2, 3, 1)[t]
+            e = int(rng.integers(k // 3, 3 * (k + 4) + 2 * k))
+            x = (rng.standard_normal(e) * 4).astype(np.float32)
+            d = tc.derate_match_llr(k, f, x, rv)
+            acc = d if acc is None else acc + d
+            tx.append((k, f, e, rv, e_off, llr_off))
+            e_parts.append(x)
+            e_off += e
+        host.append(acc)
+        llr_off += 3 * (k + 4)
+    e_llr = torch.from_numpy(np.concatenate(e_parts)).cuda()
+    out = torch.full((llr_off,), 9.0, device="cuda")
+    decoder.derate_combine_device(tx, e_llr.data_ptr(), e_llr.numel(), out.data_ptr(), llr_off)
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), np.concatenate(host))
+    with pytest.raises(tc.InvalidArgument):  # filler disagrees inside one code block's group
+        k0, f0 = tx[0][0], tx[0][1]
+        bad = [tx[0], (k0, (f0 + 8) % k0) + tx[0][2:]]
+        decoder.derate_combine_device(bad, e_llr.data_ptr(), e_llr.numel(), out.data_ptr(), llr_off)

@@ -138,6 +138,7 @@ _SIGNATURES = {
     "tc_autotune_load": [_VP, C.c_char_p],
     "tc_decoder_set_timing": [_VP, C.c_int],
     "tc_decoder_timing": [_VP, _VP, C.c_int],
+    "tc_derate_combine_llr_device": [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, _VP],
     "tc_adjoint_create": [_VP, _VP],
     "tc_adjoint_destroy": [_VP],
     "tc_adjoint_forward": [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, C.c_uint32, _VP, C.c_int32,
@@ -563,6 +564,18 @@ class Decoder:
         arr, _, _ = self.rm_blocks(blocks)
         _call("tc_derate_match_llr_device", self._h, len(blocks), C.addressof(arr), int(e_len),
               e_ptr, int(llr_len), out_ptr, stream or None)
+
+    def derate_combine_device(self, transmissions, e_ptr: int, e_len: int, out_ptr: int,
+                              llr_len: int, stream: int = 0) -> None:
+        """HARQ soft combining on the GPU: transmissions = (k, filler, e, rv, e_offset,
+        llr_offset) tuples, those of one code block consecutive with the same llr_offset; each
+        code block's [d0|d1|d2] becomes the sum of its transmissions' de-rate-matched LLRs."""
+        arr = (_RmBlock * max(len(transmissions), 1))()
+        for i, (k, f, e, rv, eo, lo) in enumerate(transmissions):
+            arr[i].k, arr[i].filler, arr[i].e, arr[i].rv = int(k), int(f), int(e), int(rv)
+            arr[i].e_offset, arr[i].llr_offset = int(eo), int(lo)
+        _call("tc_derate_combine_llr_device", self._h, len(transmissions), C.addressof(arr),
+              int(e_len), e_ptr, int(llr_len), out_ptr, stream or None)
 
     def decode_tbs(self, tbs, blocks, e_llr, options: Optional[DecodeOptions] = None,
                    want_posterior: bool = False):

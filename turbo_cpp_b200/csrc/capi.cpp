@@ -392,6 +392,16 @@ int tc_derate_match_llr_device(tc_decoder* dec, size_t n_cb, const tc_rm_block* 
   });
 }
 
+int tc_derate_combine_llr_device(tc_decoder* dec, size_t n_tx, const tc_rm_block* tx,
+                                 size_t e_len, const float* e_llr, size_t llr_len, float* d012,
+                                 void* stream) {
+  return guarded([&] {
+    need(dec != nullptr && (n_tx == 0 || (tx && e_llr && d012)), "null pointer");
+    dec->impl.derate_combine_llr(n_tx, reinterpret_cast<const tcb::RmBlockDesc*>(tx), e_llr,
+                                 e_len, d012, llr_len, stream);
+  });
+}
+
 int tc_decode_transport_blocks(tc_decoder* dec, size_t n_tb, const tc_transport_block* tbs,
                                size_t n_cb, const tc_rm_block* cbs, size_t e_len,
                                const float* e_llr, size_t bits_len, uint8_t* tb_bits,

@@ -111,6 +111,78 @@ __global__ void __launch_bounds__(kRmThreads) derate_llr_kernel(const DevRm* __r
   }
 }
 
+// HARQ soft combining: one CTA per code block, whose transmissions (up to kMaxHarqTx, each with
+// its own rv, E and rate-matched LLRs) are consecutive in `tx`.  The ranks of the valid
+// circular-buffer positions depend only on K and the filler count, so one scan serves every
+// transmission; each stream element sums each transmission's visits in increasing k from 0.0f
+// (that transmission's de-rate-matched value, as derate_llr_kernel) and adds the transmissions
+// in their order -- bit-identical to de-rate matching each transmission alone and adding the
+// results in that order.
+constexpr int kMaxHarqTx = 8;
+
+__global__ void __launch_bounds__(kRmThreads) derate_combine_kernel(
+    const DevRm* __restrict__ tx, const int32_t* __restrict__ group_first,
+    const float* __restrict__ e_llr, float* __restrict__ d012) {
+  __shared__ int warp_sum[kRmThreads / 32];
+  __shared__ int s_rank_k0[kMaxHarqTx], s_total;
+  const int t0 = group_first[blockIdx.x], nt = group_first[blockIdx.x + 1] - t0;
+  const DevRm b = tx[t0];
+  const int d = b.k + 4, rows = (d + 31) / 32, kpi = rows * 32, ncb = 3 * kpi;
+  float* out = d012 + b.out;
+  for (int i = threadIdx.x; i < 3 * d; i += blockDim.x) out[i] = 0.0f;
+  const int chunk = (ncb + blockDim.x - 1) / blockDim.x;
+  const int p0 = min(ncb, static_cast<int>(threadIdx.x) * chunk), p1 = min(ncb, p0 + chunk);
+  int cnt = 0;
+  for (int p = p0; p < p1; ++p) cnt += rm_source(p, d, rows, kpi, b.filler) >= 0;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) warp_sum[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    int v = lane < kRmThreads / 32 ? warp_sum[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += u;
+    }
+    if (lane < kRmThreads / 32) warp_sum[lane] = v;
+  }
+  __syncthreads();
+  const int before = (wid ? warp_sum[wid - 1] : 0) + incl - cnt;
+  if (threadIdx.x == blockDim.x - 1) s_total = before + cnt;
+  for (int t = 0; t < nt; ++t) {
+    const int k0 = rows * (2 * ((ncb + 8 * rows - 1) / (8 * rows)) * tx[t0 + t].rv + 2) % ncb;
+    if (k0 >= p0 && k0 < p1) {
+      int r = before;
+      for (int p = p0; p < k0; ++p) r += rm_source(p, d, rows, kpi, b.filler) >= 0;
+      s_rank_k0[t] = r;
+    }
+  }
+  __syncthreads();  // also orders the zero fill before the scattered writes
+  const int nv = s_total;
+  int rank = before;
+  for (int p = p0; p < p1; ++p) {
+    const int src = rm_source(p, d, rows, kpi, b.filler);
+    if (src < 0) continue;
+    float acc = 0.0f;
+    for (int t = 0; t < nt; ++t) {
+      const DevRm& x = tx[t0 + t];
+      int kk = rank - s_rank_k0[t];
+      if (kk < 0) kk += nv;
+      float part = 0.0f;
+      for (; kk < x.e; kk += nv) part += e_llr[x.e_off + kk];
+      acc += part;
+    }
+    out[src] = acc;
+    ++rank;
+  }
+}
+
 struct DevTb {
   int32_t first_cb, n_cb;
   int64_t tbs;       // transport block size without CRC24A
@@ -193,6 +265,48 @@ void Decoder::derate_device(size_t n, const RmBlockDesc* blocks, const float* e_
       d, e_llr, d012);
   check(cudaGetLastError(), "de-rate launch");
   timing_.launches += 1;
+}
+
+// HARQ combining: transmissions of one code block are consecutive entries with the same
+// llr_offset (and K, filler); each group's [d0|d1|d2] becomes the sum of its transmissions'
+// de-rate-matched LLRs.
+void Decoder::derate_combine_llr(size_t n, const RmBlockDesc* tx, const float* e_llr, size_t e_len,
+                                 float* d012, size_t llr_len, void* stream) {
+  std::lock_guard<std::mutex> lock(mu_);
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  std::vector<DevRm> v(n);
+  std::vector<int32_t> first;
+  for (size_t i = 0; i < n; ++i) {
+    const RmBlockDesc& b = tx[i];
+    if (qpp_index(b.k) < 0) throw OutOfRange("unsupported QPP block size");
+    if (b.filler < 0 || b.filler >= b.k || b.rv > 3 || b.e < 0)
+      throw InvalidArgument("invalid filler count, rv or E");
+    if (b.e_offset < 0 || static_cast<size_t>(b.e_offset) + static_cast<size_t>(b.e) > e_len)
+      throw InvalidArgument("rate-matched LLRs out of range");
+    if (b.llr_offset < 0 || b.llr_offset % 4 != 0 ||
+        static_cast<size_t>(b.llr_offset) + 3 * static_cast<size_t>(b.k + 4) > llr_len)
+      throw InvalidArgument("invalid LLR offset (must be a multiple of 4 and in range)");
+    const bool same = i > 0 && b.llr_offset == tx[i - 1].llr_offset;
+    if (same && (b.k != tx[i - 1].k || b.filler != tx[i - 1].filler))
+      throw InvalidArgument("transmissions of one code block must agree on K and filler");
+    if (!same) first.push_back(static_cast<int32_t>(i));
+    else if (static_cast<int>(i) - first.back() >= kMaxHarqTx)
+      throw InvalidArgument("at most 8 transmissions per code block");
+    v[i] = DevRm{b.k, b.filler, b.e, static_cast<int32_t>(b.rv), b.e_offset, b.llr_offset};
+  }
+  if (n == 0) return;
+  const size_t groups = first.size();
+  first.push_back(static_cast<int32_t>(n));
+  order_after_previous(stream);
+  DevRm* d = grow<DevRm>(d_rm_, n);
+  int32_t* g = grow<int32_t>(d_rmgroup_, groups + 1);
+  upload(d, v.data(), n * sizeof(DevRm), stream);
+  upload(g, first.data(), (groups + 1) * sizeof(int32_t), stream);
+  derate_combine_kernel<<<static_cast<unsigned>(groups), kRmThreads, 0,
+                          static_cast<cudaStream_t>(stream)>>>(d, g, e_llr, d012);
+  check(cudaGetLastError(), "combine launch");
+  timing_.launches += 1;
+  mark_done(stream);
 }
 
 void Decoder::derate_match_llr(size_t n, const RmBlockDesc* blocks, const float* e_llr,

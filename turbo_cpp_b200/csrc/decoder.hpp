@@ -152,6 +152,9 @@ class Decoder {
   void derate_match_llr(size_t n, const RmBlockDesc* blocks, const float* e_llr, size_t e_len,
                         float* d012, size_t llr_len, void* stream);
   void decode_transport_blocks(const TbRequest& q);
+  // HARQ soft combining of several transmissions (redundancy versions) per code block
+  void derate_combine_llr(size_t n, const RmBlockDesc* tx, const float* e_llr, size_t e_len,
+                          float* d012, size_t llr_len, void* stream);
   int sm_count() const { return sm_count_; }
 
   // QPP tables on the device (uint16 per position; all 188 sizes back to back) and the offset
@@ -221,6 +224,7 @@ class Decoder {
   DeviceBuffer d_perm_, d_inv_, d_xpow_;
   DeviceBuffer d_cbs_, d_wincb_, d_start_, d_llr_, d_sysi_, d_e1i_, d_e2_, d_post_, d_seed_,
       d_done_, d_iters_, d_crc_, d_ckpt_, d_tasks_, d_queue_;
+  DeviceBuffer d_rmgroup_;
   DeviceBuffer d_rm_, d_e_llr_, d_d012_, d_tbpost_, d_tbbits_, d_tbok_, d_cbok_, d_tbiters_, d_tb_,
       d_xpow_a_;
   int persist_blocks_per_sm_ = 0;
