@@ -188,6 +188,27 @@ TC_API int tc_derate_match_llr_device(tc_decoder* dec, size_t n_cb, const tc_rm_
                                       size_t e_len, const float* e_llr, size_t llr_len,
                                       float* d012, void* stream);
 
+/* ---------------- test-vector generation on the device (new) ----------------
+ * tc_awgn_code_blocks_device: the device version of tc_awgn_code_blocks (same seed, same
+ * layout: K information bits per block back to back in `bits`, [d0|d1|d2] LLRs per block back
+ * to back in `llr`, both device memory; k, filler (may be NULL: none) and ebn0_db are host
+ * arrays of n).  Bits (and their CRC24B) and encoded streams are bit-identical to the host
+ * generator; the LLRs are equal up to the last bit of double log/cos on the device against the
+ * host C library.  tc_turbo_encode_device: turbo_encode_code_block (lte_turbo.cpp:624-688) of
+ * many blocks (bits in, 3(K+4) encoded bits per block out, back to back, device memory).
+ * tc_rate_match_device: rate matching (lte_turbo.cpp:250-278) of many blocks: tc_rm_block
+ * gives K, filler, E, rv, the output offset (e_offset) and the offset of the block's encoded
+ * [d0|d1|d2] bits in d012 (llr_offset).  All ordered on `stream`. */
+TC_API int tc_awgn_code_blocks_device(tc_decoder* dec, uint64_t seed, size_t n, const int32_t* k,
+                                      const int32_t* filler, const float* ebn0_db, int crc24b,
+                                      uint8_t* bits, float* llr, void* stream);
+TC_API int tc_turbo_encode_device(tc_decoder* dec, size_t n, const int32_t* k,
+                                  const int32_t* filler, const uint8_t* bits, uint8_t* d012,
+                                  void* stream);
+TC_API int tc_rate_match_device(tc_decoder* dec, size_t n, const tc_rm_block* blocks,
+                                size_t d012_len, const uint8_t* d012, size_t e_len,
+                                uint8_t* e_bits, void* stream);
+
 /* HARQ soft combining (new; the reference de-rate matches a single transmission,
  * lte_turbo.cpp:280-325): the n_tx entries of tx are transmissions; those of one code block are
  * consecutive and share llr_offset, K and filler (at most 8 per code block), each with its own

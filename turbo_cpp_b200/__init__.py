@@ -139,6 +139,9 @@ _SIGNATURES = {
     "tc_decoder_set_timing": [_VP, C.c_int],
     "tc_decoder_timing": [_VP, _VP, C.c_int],
     "tc_derate_combine_llr_device": [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, _VP],
+    "tc_awgn_code_blocks_device": [_VP, _U64, _SZ, _VP, _VP, _VP, C.c_int, _VP, _VP, _VP],
+    "tc_turbo_encode_device": [_VP, _SZ, _VP, _VP, _VP, _VP, _VP],
+    "tc_rate_match_device": [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, _VP],
     "tc_adjoint_create": [_VP, _VP],
     "tc_adjoint_destroy": [_VP],
     "tc_adjoint_forward": [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, C.c_uint32, _VP, C.c_int32,
@@ -484,6 +487,7 @@ class Decoder:
         h = C.c_void_p()
         _call("tc_decoder_create", int(device), C.addressof(h))
         self._h = h
+        self.device = int(device)
 
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:
@@ -564,6 +568,48 @@ class Decoder:
         arr, _, _ = self.rm_blocks(blocks)
         _call("tc_derate_match_llr_device", self._h, len(blocks), C.addressof(arr), int(e_len),
               e_ptr, int(llr_len), out_ptr, stream or None)
+
+    # -- test-vector generation on the device (torch CUDA tensors out) --
+    def awgn_code_blocks_device(self, seed: int, ks, ebn0_db, fillers=None, crc24b: bool = False,
+                                stream: int = 0):
+        """The device version of awgn_code_blocks: returns (bits uint8, LLRs float32) as CUDA
+        tensors in the same layout, bits identical to the host generator's."""
+        import torch
+
+        ks = np.ascontiguousarray(ks, np.int32)
+        n = ks.size
+        f = np.zeros(n, np.int32) if fillers is None else np.ascontiguousarray(fillers, np.int32)
+        eb = np.ascontiguousarray(np.broadcast_to(np.asarray(ebn0_db, np.float32), (n,)))
+        dev = torch.device("cuda", self.device)
+        bits = torch.empty(int(ks.sum()), dtype=torch.uint8, device=dev)
+        llr = torch.empty(int(3 * (ks.astype(np.int64) + 4).sum()), dtype=torch.float32, device=dev)
+        _call("tc_awgn_code_blocks_device", self._h, int(seed), n, _ptr(ks), _ptr(f), _ptr(eb),
+              int(bool(crc24b)), bits.data_ptr(), llr.data_ptr(), stream or None)
+        return bits, llr
+
+    def turbo_encode_device(self, ks, bits, fillers=None, stream: int = 0):
+        """Encodes blocks stored back to back in the CUDA uint8 tensor `bits`; returns their
+        [d0|d1|d2] bits back to back (CUDA uint8 tensor)."""
+        import torch
+
+        ks = np.ascontiguousarray(ks, np.int32)
+        f = np.zeros(ks.size, np.int32) if fillers is None else np.ascontiguousarray(fillers, np.int32)
+        d = torch.empty(int(3 * (ks.astype(np.int64) + 4).sum()), dtype=torch.uint8,
+                        device=bits.device)
+        _call("tc_turbo_encode_device", self._h, ks.size, _ptr(ks), _ptr(f), bits.data_ptr(),
+              d.data_ptr(), stream or None)
+        return d
+
+    def rate_match_device(self, blocks, d012, stream: int = 0):
+        """blocks = (k, filler, e, rv) per block, encoded bits back to back in the CUDA uint8
+        tensor d012; returns the E rate-matched bits per block back to back."""
+        import torch
+
+        arr, e_len, d_len = self.rm_blocks(blocks)
+        out = torch.empty(max(e_len, 1), dtype=torch.uint8, device=d012.device)
+        _call("tc_rate_match_device", self._h, len(blocks), C.addressof(arr), int(d012.numel()),
+              d012.data_ptr(), int(e_len), out.data_ptr(), stream or None)
+        return out[:e_len]
 
     def derate_combine_device(self, transmissions, e_ptr: int, e_len: int, out_ptr: int,
                               llr_len: int, stream: int = 0) -> None:

@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libturbo_b200.so")
-SOURCES = ["decoder.cu", "chain.cu", "noalloc.cu", "adjoint.cu", "lte_codec.cpp", "capi.cpp"]
+SOURCES = ["decoder.cu", "chain.cu", "noalloc.cu", "adjoint.cu", "generate.cu", "lte_codec.cpp", "capi.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

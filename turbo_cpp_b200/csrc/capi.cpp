@@ -4,6 +4,7 @@
 #include <exception>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/turbo_b200.h"
 #include "adjoint.hpp"
@@ -389,6 +390,37 @@ int tc_derate_match_llr_device(tc_decoder* dec, size_t n_cb, const tc_rm_block* 
     static_assert(sizeof(tc_rm_block) == sizeof(tcb::RmBlockDesc), "descriptor layout");
     dec->impl.derate_match_llr(n_cb, reinterpret_cast<const tcb::RmBlockDesc*>(blocks), e_llr,
                                e_len, d012, llr_len, stream);
+  });
+}
+
+int tc_awgn_code_blocks_device(tc_decoder* dec, uint64_t seed, size_t n, const int32_t* k,
+                               const int32_t* filler, const float* ebn0_db, int crc24b,
+                               uint8_t* bits, float* llr, void* stream) {
+  return guarded([&] {
+    need(dec != nullptr && (n == 0 || (k && ebn0_db && bits && llr)), "null pointer");
+    std::vector<int32_t> f(n, 0);
+    if (filler) f.assign(filler, filler + n);
+    dec->impl.awgn_code_blocks_device(seed, n, k, f.data(), ebn0_db, crc24b != 0, bits, llr,
+                                      stream);
+  });
+}
+
+int tc_turbo_encode_device(tc_decoder* dec, size_t n, const int32_t* k, const int32_t* filler,
+                           const uint8_t* bits, uint8_t* d012, void* stream) {
+  return guarded([&] {
+    need(dec != nullptr && (n == 0 || (k && bits && d012)), "null pointer");
+    std::vector<int32_t> f(n, 0);
+    if (filler) f.assign(filler, filler + n);
+    dec->impl.turbo_encode_device(n, k, f.data(), bits, d012, stream);
+  });
+}
+
+int tc_rate_match_device(tc_decoder* dec, size_t n, const tc_rm_block* blocks, size_t d012_len,
+                         const uint8_t* d012, size_t e_len, uint8_t* e_bits, void* stream) {
+  return guarded([&] {
+    need(dec != nullptr && (n == 0 || (blocks && d012 && e_bits)), "null pointer");
+    dec->impl.rate_match_device(n, reinterpret_cast<const tcb::RmBlockDesc*>(blocks), d012,
+                                d012_len, e_bits, e_len, stream);
   });
 }
 

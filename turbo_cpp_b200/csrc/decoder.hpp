@@ -152,6 +152,15 @@ class Decoder {
   void derate_match_llr(size_t n, const RmBlockDesc* blocks, const float* e_llr, size_t e_len,
                         float* d012, size_t llr_len, void* stream);
   void decode_transport_blocks(const TbRequest& q);
+  // test-vector generation on the device (generate.cu): the host generator's seeded bits
+  // (+ CRC24B), encoder and channel; the encoder and the rate matcher alone
+  void awgn_code_blocks_device(uint64_t seed, size_t n, const int32_t* k, const int32_t* filler,
+                               const float* ebn0_db, bool crc24b, uint8_t* bits, float* llr,
+                               void* stream);
+  void turbo_encode_device(size_t n, const int32_t* k, const int32_t* filler, const uint8_t* bits,
+                           uint8_t* d012, void* stream);
+  void rate_match_device(size_t n, const RmBlockDesc* blocks, const uint8_t* d012,
+                         size_t d012_len, uint8_t* e_bits, size_t e_len, void* stream);
   // HARQ soft combining of several transmissions (redundancy versions) per code block
   void derate_combine_llr(size_t n, const RmBlockDesc* tx, const float* e_llr, size_t e_len,
                           float* d012, size_t llr_len, void* stream);
@@ -224,7 +233,7 @@ class Decoder {
   DeviceBuffer d_perm_, d_inv_, d_xpow_;
   DeviceBuffer d_cbs_, d_wincb_, d_start_, d_llr_, d_sysi_, d_e1i_, d_e2_, d_post_, d_seed_,
       d_done_, d_iters_, d_crc_, d_ckpt_, d_tasks_, d_queue_;
-  DeviceBuffer d_rmgroup_;
+  DeviceBuffer d_rmgroup_, d_gen_, d_gentab_, d_genenc_, d_genrm_;
   DeviceBuffer d_rm_, d_e_llr_, d_d012_, d_tbpost_, d_tbbits_, d_tbok_, d_cbok_, d_tbiters_, d_tb_,
       d_xpow_a_;
   int persist_blocks_per_sm_ = 0;

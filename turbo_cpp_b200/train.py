@@ -1,8 +1,8 @@
 """Scale-training harness: learns the 2 per-iteration extrinsic scale factors of the unrolled
 Log-MAP turbo decoder by Adam on the mean binary cross-entropy of the posterior LLRs against the
 true information bits, with gradients from the hand-written adjoint.  Every step decodes a
-freshly seeded batch (seed + step): BPSK over AWGN at a fixed Eb/N0, rate 1/3 with tails.
-The host builds the next batch while the GPU runs the current step.
+freshly seeded batch (seed + step): BPSK over AWGN at a fixed Eb/N0, rate 1/3 with tails,
+generated on the GPU (the same bits and LLRs as the host generator for the same seed).
 
     python -m turbo_cpp_b200.train --steps 200 --blocks 1024 --k 6144 --ebn0 0.6 \\
         --iterations 6 --out scales.json
@@ -12,7 +12,6 @@ from __future__ import annotations
 import argparse
 import json
 import time
-from concurrent.futures import ThreadPoolExecutor
 from typing import Callable, Optional
 
 import numpy as np
@@ -22,12 +21,14 @@ def train_scales(steps: int = 200, n_blocks: int = 1024, k: int = 6144, ebn0_db:
                  iterations: int = 6, lr: float = 0.01, seed: int = 4000, window: int = 0,
                  guard: int = -1, device: int = 0,
                  callback: Optional[Callable[[dict], None]] = None):
-    """Returns (trained scales as a float32 array of 2*iterations, per-step history).  The
-    learning rate decays from lr to lr/10 over the run (cosine)."""
+    """Returns (trained scales as a float32 array of 2*iterations, per-step history, held-out
+    record).  The learning rate decays from lr to lr/10 over the run (cosine, one scheduler
+    step per Adam step).  The held-out record is the loss / BER / BLER of one fixed batch
+    (seed + 1000000) with the initial scales (all 1) and with the trained ones: the training
+    batches are too noisy to show progress."""
     import torch
     import torch.nn.functional as F
 
-    from . import awgn_code_blocks
     from .autograd import DifferentiableDecoder
 
     dev = torch.device("cuda", device)
@@ -39,15 +40,11 @@ def train_scales(steps: int = 200, n_blocks: int = 1024, k: int = 6144, ebn0_db:
     # moving by about lr around their optimum
     sched = torch.optim.lr_scheduler.LambdaLR(
         opt, lambda i: 0.1 + 0.45 * (1.0 + np.cos(np.pi * min(i, steps) / max(steps, 1))))
-    # cosine decay to lr/10: the batch-to-batch noise of the loss otherwise keeps the scales
-    # moving by about lr around their optimum
-    sched = torch.optim.lr_scheduler.LambdaLR(
-        opt, lambda i: 0.1 + 0.45 * (1.0 + np.cos(np.pi * min(i, steps) / max(steps, 1))))
     history = []
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    vbits, vllr = awgn_code_blocks(seed + 1000000, ks, ebn0_db)
-    vx = torch.from_numpy(vllr).to(dev)
-    vb = torch.from_numpy(vbits).to(dev, torch.float32)
+    gen = dd.decoder.awgn_code_blocks_device
+    vbits, vx = gen(seed + 1000000, ks, ebn0_db)
+    vb = vbits.to(torch.float32)
 
     def held_out(sc):
         with torch.no_grad():
@@ -57,31 +54,26 @@ def train_scales(steps: int = 200, n_blocks: int = 1024, k: int = 6144, ebn0_db:
                         ber=float(errs.mean()), bler=float(errs.amax(1).mean()))
 
     held = {"initial": held_out(scales.detach())}
-    with ThreadPoolExecutor(1) as pool:
-        fut = pool.submit(awgn_code_blocks, seed, ks, ebn0_db)
-        for step in range(steps):
-            bits, llr = fut.result()
-            if step + 1 < steps:
-                fut = pool.submit(awgn_code_blocks, seed + step + 1, ks, ebn0_db)
-            x = torch.from_numpy(llr).to(dev)
-            b = torch.from_numpy(bits).to(dev, torch.float32)
-            ev[0].record()
-            post = dd(x, scales)
-            loss = F.binary_cross_entropy_with_logits(post, b)
-            opt.zero_grad(set_to_none=True)
-            loss.backward()
-            ev[1].record()
-            opt.step()
-            sched.step()
-            sched.step()
-            with torch.no_grad():
-                errs = ((post >= 0).float() != b).float().view(n_blocks, k)
-            rec = dict(step=step, loss=float(loss.detach()), ber=float(errs.mean()),
-                       bler=float(errs.amax(1).mean()), ms=ev[0].elapsed_time(ev[1]),
-                       scales=[float(v) for v in scales.detach().cpu()])
-            history.append(rec)
-            if callback:
-                callback(rec)
+    for step in range(steps):
+        bits, x = gen(seed + step, ks, ebn0_db)
+        b = bits.to(torch.float32)
+        ev[0].record()
+        post = dd(x, scales)
+        loss = F.binary_cross_entropy_with_logits(post, b)
+        opt.zero_grad(set_to_none=True)
+        loss.backward()
+        ev[1].record()
+        opt.step()
+        sched.step()
+        with torch.no_grad():
+            errs = ((post >= 0).float() != b).float().view(n_blocks, k)
+        rec = dict(step=step, lr=float(opt.param_groups[0]["lr"]), loss=float(loss.detach()),
+                   ber=float(errs.mean()),
+                   bler=float(errs.amax(1).mean()), ms=ev[0].elapsed_time(ev[1]),
+                   scales=[float(v) for v in scales.detach().cpu()])
+        history.append(rec)
+        if callback:
+            callback(rec)
     held["trained"] = held_out(scales.detach())
     return scales.detach().cpu().numpy().astype(np.float32), history, held
 
