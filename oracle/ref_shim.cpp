@@ -114,6 +114,25 @@ int ref_turbo_encode(std::int32_t k, std::int32_t filler, const std::uint8_t* cb
   }
 }
 
+// The reference encoder's tail arrays (EncodedCodeBlock upper/lower tail systematic/parity,
+// lte_turbo.cpp:655-685) in that order, 3 bytes each.
+int ref_turbo_encode_tails(std::int32_t k, std::int32_t filler, const std::uint8_t* cb,
+                           std::uint8_t* tails) {
+  try {
+    const auto e = turbo_encode_code_block(make_desc(k, filler),
+                                           std::span<const std::uint8_t>(cb, k));
+    for (int i = 0; i < 3; ++i) {
+      tails[i] = e.upper_tail_systematic[i];
+      tails[3 + i] = e.upper_tail_parity[i];
+      tails[6 + i] = e.lower_tail_systematic[i];
+      tails[9 + i] = e.lower_tail_parity[i];
+    }
+    return 0;
+  } catch (const std::exception&) {
+    return -1;
+  }
+}
+
 // Full transport-block encode.  Per code block r: cb_k[r], cb_filler[r], cb_e[r]; the rate
 // matched bits of all blocks back to back in rm_out (capacity rm_cap).
 int ref_encode_tb(std::size_t tbs, std::size_t g_total, std::uint32_t rv, std::uint32_t nl,
