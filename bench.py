@@ -614,12 +614,19 @@ def main():
             "avg_launch_ms": avg_launch_ms,
             "peak_source": f"{props.multi_processor_count} SMs x {MUFU_PER_SM_CLK} MUFU/clk x "
                            f"median sampled SM clock {sm_mhz:.0f} MHz (nominal issue rate)",
+            "note": "the binding roofline is the SFU (MUFU ex2/lg2 of the exact max*); the "
+                    "trellis is not a contraction (no tensor cores) and HBM runs well below its "
+                    "measured peak (roofline_hbm)",
         },
         "roofline_hbm": {
             "bound": "hbm", "achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
             "frac": hbm_achieved / hbm_peak, "peak_source": f"{hbm_src} MEASURED_PEAKS hbm_gbs",
+            "traffic": None if traffic_per_step is None else traffic_per_step * steps_per_launch,
+            "dram_gbs": None if traffic_per_step is None
+            else traffic_per_step * steps_per_launch / (avg_launch_ms / 1e3) / 1e9,
             "work": "16.0 B per info bit per decode (3(K+4) LLRs in, K posteriors out), the "
-                    "launch's share",
+                    "launch's share; dram_gbs = the ncu DRAM bytes of a launch over its "
+                    "CUDA-event time (the working set streams from DRAM every half-iteration)",
         },
         "gpu_launches": int(launches),
         "clocks": clocks,
