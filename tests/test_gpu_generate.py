@@ -63,3 +63,14 @@ def test_device_encoder_and_rate_matcher_match_host(tc, decoder):
         ref.append(tc.rate_match(k, f, host[pos:pos + 3 * (k + 4)], e, rv))
         pos += 3 * (k + 4)
     assert np.array_equal(out, np.concatenate(ref))
+
+
+def test_generation_argument_errors(tc, decoder):
+    import torch
+
+    with pytest.raises(tc.OutOfRange):
+        decoder.awgn_code_blocks_device(1, [44], 1.0)
+    with pytest.raises(tc.InvalidArgument):  # no room for the CRC24B after the filler
+        decoder.awgn_code_blocks_device(1, [40], 1.0, [24], crc24b=True)
+    with pytest.raises(tc.InvalidArgument):  # rate-matched output outside the buffer
+        decoder.rate_match_device([(40, 0, -1, 0)], torch.zeros(132, dtype=torch.uint8).cuda())

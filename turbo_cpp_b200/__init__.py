@@ -87,6 +87,15 @@ class _RmBlock(C.Structure):
                 ("e_offset", C.c_int64), ("llr_offset", C.c_int64)]
 
 
+# numpy views of the descriptor structs (same field order, sizes and alignment)
+_CODE_BLOCK_DTYPE = np.dtype([("k", np.int32), ("filler", np.int32), ("llr_offset", np.int64),
+                              ("out_offset", np.int64)])
+_RM_BLOCK_DTYPE = np.dtype([("k", np.int32), ("filler", np.int32), ("e", np.int32),
+                            ("rv", np.uint32), ("e_offset", np.int64), ("llr_offset", np.int64)])
+assert _CODE_BLOCK_DTYPE.itemsize == C.sizeof(_CodeBlock)
+assert _RM_BLOCK_DTYPE.itemsize == C.sizeof(_RmBlock)
+
+
 class _TransportBlock(C.Structure):
     _fields_ = [("tbs", C.c_int64), ("first_cb", C.c_int32), ("n_cb", C.c_int32),
                 ("bits_offset", C.c_int64)]
@@ -553,14 +562,15 @@ class Decoder:
     def rm_blocks(blocks):
         """tc_rm_block array from (k, filler, e, rv) tuples; E LLRs back to back, outputs
         [d0|d1|d2] back to back."""
-        arr = (_RmBlock * max(len(blocks), 1))()
-        e_off = llr_off = 0
-        for i, (k, f, e, rv) in enumerate(blocks):
-            arr[i].k, arr[i].filler, arr[i].e, arr[i].rv = int(k), int(f), int(e), int(rv)
-            arr[i].e_offset, arr[i].llr_offset = e_off, llr_off
-            e_off += int(e)
-            llr_off += 3 * (int(k) + 4)
-        return arr, e_off, llr_off
+        b = np.asarray(blocks, np.int64).reshape(-1, 4)
+        n = b.shape[0]
+        e_off = np.concatenate([[0], np.cumsum(b[:, 2])])
+        llr_off = np.concatenate([[0], np.cumsum(3 * (b[:, 0] + 4))])
+        rec = np.zeros(max(n, 1), dtype=_RM_BLOCK_DTYPE)
+        rec["k"][:n], rec["filler"][:n], rec["e"][:n], rec["rv"][:n] = b[:, 0], b[:, 1], b[:, 2], b[:, 3]
+        rec["e_offset"][:n], rec["llr_offset"][:n] = e_off[:-1], llr_off[:-1]
+        arr = (_RmBlock * max(n, 1)).from_buffer(rec)  # shares (and keeps) rec's memory
+        return arr, int(e_off[-1]), int(llr_off[-1])
 
     def derate_device(self, blocks, e_ptr: int, e_len: int, out_ptr: int, llr_len: int,
                       stream: int = 0) -> None:
@@ -678,14 +688,12 @@ class Decoder:
         ks = np.asarray(ks, np.int64)
         n = ks.size
         fillers = np.zeros(n, np.int64) if fillers is None else np.asarray(fillers, np.int64)
-        cbs = (_CodeBlock * max(n, 1))()
         llr_off = np.concatenate([[0], np.cumsum(3 * (ks + 4))])
         out_off = np.concatenate([[0], np.cumsum(ks)])
-        for i in range(n):
-            cbs[i].k = int(ks[i])
-            cbs[i].filler = int(fillers[i])
-            cbs[i].llr_offset = int(llr_off[i])
-            cbs[i].out_offset = int(out_off[i])
+        rec = np.zeros(max(n, 1), dtype=_CODE_BLOCK_DTYPE)
+        rec["k"][:n], rec["filler"][:n] = ks, fillers
+        rec["llr_offset"][:n], rec["out_offset"][:n] = llr_off[:-1], out_off[:-1]
+        cbs = (_CodeBlock * max(n, 1)).from_buffer(rec)  # shares (and keeps) rec's memory
         return cbs, int(llr_off[-1]), int(out_off[-1])
 
     def decode(self, ks, llr, fillers=None, options: Optional[DecodeOptions] = None):
