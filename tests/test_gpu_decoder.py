@@ -196,3 +196,33 @@ def test_config2_full_size_properties(tc, decoder, oracle):
         ref, _, _ = oracle.decode_cb(k, 0, llr[i * 3 * (k + 4):(i + 1) * 3 * (k + 4)], 8)
         err, hard = llr_close(post[i * k:(i + 1) * k], ref)
         assert err <= RTOL and hard == 0, (i, err, hard)
+
+
+def test_concurrent_calls_on_one_decoder(tc, decoder):
+    """Calls on one decoder from several host threads (the reference fans Stage 2 decodes out
+    with std::async, lte_turbo.cpp:941-951) give the results of the same calls made one by one."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    jobs = []
+    for i in range(8):
+        ks = [6144, 1024, 40 + 8 * i, 2048]
+        llr, _ = awgn_blocks(tc, ks, 0.4 + 0.1 * i, seed=300 + i)
+        jobs.append((ks, llr, tc.DecodeOptions(6, i % 2 == 1, 0, -1,
+                                               tc.SCHEDULE_PERSISTENT if i % 3 == 0 else tc.SCHEDULE_PLAIN)))
+    serial = [decoder.decode(ks, llr, options=o) for ks, llr, o in jobs]
+    with ThreadPoolExecutor(4) as pool:
+        threaded = list(pool.map(lambda j: decoder.decode(j[0], j[1], options=j[2]), jobs))
+    for a, b in zip(serial, threaded):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+
+
+def test_decoders_can_be_created_and_destroyed_repeatedly(tc):
+    llr, _ = awgn_blocks(tc, [1024], 1.0, seed=5)
+    ref = None
+    for _ in range(12):
+        d = tc.Decoder(0)
+        post, _, _ = d.decode([1024], llr)
+        ref = post if ref is None else ref
+        assert np.array_equal(post, ref)
+        d.close()
