@@ -11,6 +11,7 @@
 
 #include "decoder.hpp"
 #include "lte_codec.hpp"
+#include "circular_buffer.cuh"
 #include "siso.cuh"
 
 namespace tcb {
@@ -20,33 +21,13 @@ void check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-__constant__ uint8_t c_col_perm[32] = {0, 16, 8, 24, 4, 20, 12, 28, 2, 18, 10, 26, 6, 22, 14, 30,
-                                       1, 17, 9, 25, 5, 21, 13, 29, 3, 19, 11, 27, 7, 23, 15, 31};
-
 struct DevRm {
   int32_t k, filler, e, rv;
   int64_t e_off;  // first rate-matched LLR of the block
   int64_t out;    // float offset of [d0|d1|d2] (3(K+4) floats)
 };
 
-// Circular-buffer position -> index into [d0|d1|d2], -1 for <NULL> (sub-block interleavers of
-// lte_turbo.cpp:195-236 in closed form; interlacing lte_turbo.cpp:256-262).
-__device__ __forceinline__ int rm_source(int pos, int d, int rows, int kpi, int filler) {
-  const int dummy = kpi - d;
-  if (pos < kpi) {  // systematic, read column by column
-    const int y = (pos % rows) * 32 + c_col_perm[pos / rows] - dummy;
-    return (y < 0 || y < filler) ? -1 : y;
-  }
-  const int local = pos - kpi, lane = local >> 1;
-  if ((local & 1) == 0) {  // parity 1: same permutation as the systematic stream
-    const int y = (lane % rows) * 32 + c_col_perm[lane / rows] - dummy;
-    return (y < 0 || y < filler) ? -1 : d + y;
-  }
-  const int y = (c_col_perm[lane / rows] + 32 * (lane % rows) + 1) % kpi - dummy;
-  return y < 0 ? -1 : 2 * d + y;  // parity 2: no filler nulling
-}
-
-constexpr int kRmThreads = 512;
+constexpr int kRmThreads = kCircThreads;
 
 // One CTA per code block.  The rate-matched LLR k lands on the k-th non-<NULL> position of the
 // circular walk that starts at k0; a valid position of rank r (valid positions before it) is
@@ -59,48 +40,17 @@ __global__ void __launch_bounds__(kRmThreads) derate_llr_kernel(const DevRm* __r
   __shared__ int warp_sum[kRmThreads / 32];
   __shared__ int s_rank_k0, s_total;
   const DevRm b = blocks[blockIdx.x];
-  const int d = b.k + 4, rows = (d + 31) / 32, kpi = rows * 32, ncb = 3 * kpi;
-  const int k0 = rows * (2 * ((ncb + 8 * rows - 1) / (8 * rows)) * b.rv + 2) % ncb;
+  CircularScan cs(b.k, b.filler);
   float* out = d012 + b.out;
-  for (int i = threadIdx.x; i < 3 * d; i += blockDim.x) out[i] = 0.0f;
-  // contiguous chunk of positions per thread; count the valid ones
-  const int chunk = (ncb + blockDim.x - 1) / blockDim.x;
-  const int p0 = min(ncb, static_cast<int>(threadIdx.x) * chunk), p1 = min(ncb, p0 + chunk);
-  int cnt = 0;
-  for (int p = p0; p < p1; ++p) cnt += rm_source(p, d, rows, kpi, b.filler) >= 0;
-  // block-wide exclusive scan of the counts
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int incl = cnt;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
-  }
-  if (lane == 31) warp_sum[wid] = incl;
-  __syncthreads();
-  if (wid == 0) {
-    int v = lane < kRmThreads / 32 ? warp_sum[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int u = __shfl_up_sync(0xffffffffu, v, o);
-      if (lane >= o) v += u;
-    }
-    if (lane < kRmThreads / 32) warp_sum[lane] = v;  // inclusive per warp
-  }
-  __syncthreads();
-  const int before = (wid ? warp_sum[wid - 1] : 0) + incl - cnt;
-  if (threadIdx.x == blockDim.x - 1) s_total = before + cnt;
-  if (k0 >= p0 && k0 < p1) {
-    int r = before;
-    for (int p = p0; p < k0; ++p) r += rm_source(p, d, rows, kpi, b.filler) >= 0;
-    s_rank_k0 = r;
-  }
+  for (int i = threadIdx.x; i < 3 * cs.d; i += blockDim.x) out[i] = 0.0f;
+  cs.scan(warp_sum, &s_total);
+  cs.rank_of(cs.k0(b.rv), &s_rank_k0);
   __syncthreads();  // also orders the zero fill before the scattered writes
   const int nv = s_total, r0 = s_rank_k0;
   const float* x = e_llr + b.e_off;
-  int rank = before;
-  for (int p = p0; p < p1; ++p) {
-    const int src = rm_source(p, d, rows, kpi, b.filler);
+  int rank = cs.before;
+  for (int p = cs.p0; p < cs.p1; ++p) {
+    const int src = cs.source(p);
     if (src < 0) continue;
     int kk = rank - r0;
     if (kk < 0) kk += nv;
@@ -127,47 +77,16 @@ __global__ void __launch_bounds__(kRmThreads) derate_combine_kernel(
   __shared__ int s_rank_k0[kMaxHarqTx], s_total;
   const int t0 = group_first[blockIdx.x], nt = group_first[blockIdx.x + 1] - t0;
   const DevRm b = tx[t0];
-  const int d = b.k + 4, rows = (d + 31) / 32, kpi = rows * 32, ncb = 3 * kpi;
+  CircularScan cs(b.k, b.filler);
   float* out = d012 + b.out;
-  for (int i = threadIdx.x; i < 3 * d; i += blockDim.x) out[i] = 0.0f;
-  const int chunk = (ncb + blockDim.x - 1) / blockDim.x;
-  const int p0 = min(ncb, static_cast<int>(threadIdx.x) * chunk), p1 = min(ncb, p0 + chunk);
-  int cnt = 0;
-  for (int p = p0; p < p1; ++p) cnt += rm_source(p, d, rows, kpi, b.filler) >= 0;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int incl = cnt;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
-  }
-  if (lane == 31) warp_sum[wid] = incl;
-  __syncthreads();
-  if (wid == 0) {
-    int v = lane < kRmThreads / 32 ? warp_sum[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int u = __shfl_up_sync(0xffffffffu, v, o);
-      if (lane >= o) v += u;
-    }
-    if (lane < kRmThreads / 32) warp_sum[lane] = v;
-  }
-  __syncthreads();
-  const int before = (wid ? warp_sum[wid - 1] : 0) + incl - cnt;
-  if (threadIdx.x == blockDim.x - 1) s_total = before + cnt;
-  for (int t = 0; t < nt; ++t) {
-    const int k0 = rows * (2 * ((ncb + 8 * rows - 1) / (8 * rows)) * tx[t0 + t].rv + 2) % ncb;
-    if (k0 >= p0 && k0 < p1) {
-      int r = before;
-      for (int p = p0; p < k0; ++p) r += rm_source(p, d, rows, kpi, b.filler) >= 0;
-      s_rank_k0[t] = r;
-    }
-  }
+  for (int i = threadIdx.x; i < 3 * cs.d; i += blockDim.x) out[i] = 0.0f;
+  cs.scan(warp_sum, &s_total);
+  for (int t = 0; t < nt; ++t) cs.rank_of(cs.k0(tx[t0 + t].rv), &s_rank_k0[t]);
   __syncthreads();  // also orders the zero fill before the scattered writes
   const int nv = s_total;
-  int rank = before;
-  for (int p = p0; p < p1; ++p) {
-    const int src = rm_source(p, d, rows, kpi, b.filler);
+  int rank = cs.before;
+  for (int p = cs.p0; p < cs.p1; ++p) {
+    const int src = cs.source(p);
     if (src < 0) continue;
     float acc = 0.0f;
     for (int t = 0; t < nt; ++t) {

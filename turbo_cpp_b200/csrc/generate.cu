@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "circular_buffer.cuh"
 #include "decoder.hpp"
 #include "lte_codec.hpp"
 
@@ -158,25 +159,7 @@ __global__ void __launch_bounds__(kGenThreads) awgn_kernel(const GenBlock* __res
   }
 }
 
-constexpr int kRmGenThreads = 512;
-__constant__ uint8_t c_col_perm_g[32] = {0, 16, 8, 24, 4, 20, 12, 28, 2, 18, 10, 26, 6, 22, 14, 30,
-                                         1, 17, 9, 25, 5, 21, 13, 29, 3, 19, 11, 27, 7, 23, 15, 31};
-
-// Circular-buffer position -> index into [d0|d1|d2], -1 for <NULL> (lte_turbo.cpp:195-262).
-__device__ __forceinline__ int rm_src(int pos, int d, int rows, int kpi, int filler) {
-  const int dummy = kpi - d;
-  if (pos < kpi) {
-    const int y = (pos % rows) * 32 + c_col_perm_g[pos / rows] - dummy;
-    return (y < 0 || y < filler) ? -1 : y;
-  }
-  const int local = pos - kpi, lane = local >> 1;
-  if ((local & 1) == 0) {
-    const int y = (lane % rows) * 32 + c_col_perm_g[lane / rows] - dummy;
-    return (y < 0 || y < filler) ? -1 : d + y;
-  }
-  const int y = (c_col_perm_g[lane / rows] + 32 * (lane % rows) + 1) % kpi - dummy;
-  return y < 0 ? -1 : 2 * d + y;
-}
+constexpr int kRmGenThreads = kCircThreads;
 
 struct RmGen {
   int32_t k, filler, e, rv;
@@ -191,45 +174,16 @@ __global__ void __launch_bounds__(kRmGenThreads) rate_match_kernel(const RmGen* 
   __shared__ int warp_sum[kRmGenThreads / 32];
   __shared__ int s_rank_k0, s_total;
   const RmGen b = blocks[blockIdx.x];
-  const int d = b.k + 4, rows = (d + 31) / 32, kpi = rows * 32, ncb = 3 * kpi;
-  const int k0 = rows * (2 * ((ncb + 8 * rows - 1) / (8 * rows)) * b.rv + 2) % ncb;
-  const int chunk = (ncb + blockDim.x - 1) / blockDim.x;
-  const int p0 = min(ncb, static_cast<int>(threadIdx.x) * chunk), p1 = min(ncb, p0 + chunk);
-  int cnt = 0;
-  for (int p = p0; p < p1; ++p) cnt += rm_src(p, d, rows, kpi, b.filler) >= 0;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int incl = cnt;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
-  }
-  if (lane == 31) warp_sum[wid] = incl;
-  __syncthreads();
-  if (wid == 0) {
-    int v = lane < kRmGenThreads / 32 ? warp_sum[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int u = __shfl_up_sync(0xffffffffu, v, o);
-      if (lane >= o) v += u;
-    }
-    if (lane < kRmGenThreads / 32) warp_sum[lane] = v;
-  }
-  __syncthreads();
-  const int before = (wid ? warp_sum[wid - 1] : 0) + incl - cnt;
-  if (threadIdx.x == blockDim.x - 1) s_total = before + cnt;
-  if (k0 >= p0 && k0 < p1) {
-    int r = before;
-    for (int p = p0; p < k0; ++p) r += rm_src(p, d, rows, kpi, b.filler) >= 0;
-    s_rank_k0 = r;
-  }
+  CircularScan cs(b.k, b.filler);
+  cs.scan(warp_sum, &s_total);
+  cs.rank_of(cs.k0(b.rv), &s_rank_k0);
   __syncthreads();
   const int nv = s_total, r0 = s_rank_k0;
   const uint8_t* src_bits = d012 + b.d_off;
   uint8_t* out = e_bits + b.e_off;
-  int rank = before;
-  for (int p = p0; p < p1; ++p) {
-    const int src = rm_src(p, d, rows, kpi, b.filler);
+  int rank = cs.before;
+  for (int p = cs.p0; p < cs.p1; ++p) {
+    const int src = cs.source(p);
     if (src < 0) continue;
     int kk = rank - r0;
     if (kk < 0) kk += nv;
