@@ -307,16 +307,34 @@ Decoder::TuneChoice Decoder::autotune(const DecodeRequest& rq_in) {
     bool persistent;
     int window;
   };
-  const Cand cands[] = {{false, 128}, {false, 144}, {false, 160}, {false, 168}, {false, 176},
-                        {false, 192}, {false, 224}, {false, 256}, {true, 192}, {true, 256},
-                        {true, 320}};
+  std::vector<Cand> cands = {{false, 128}, {false, 144}, {false, 160}, {false, 168},
+                             {false, 176}, {false, 192}, {false, 224}, {false, 256},
+                             {true, 192},  {true, 256},  {true, 320}};
+  const int guard = rq_in.guard < 0 ? kDefaultGuard : rq_in.guard;
+  // Plain-schedule windows that fill whole waves: the smallest window (a multiple of 8, at
+  // least the guard) whose windows over all blocks fit in j resident waves of the SISO kernel
+  // (SMs x blocks per SM x threads per block), for j = 2, 3, 4.  A launch with a partly filled
+  // last wave idles SMs for the length of a window (measured at 4096 x K=6144: window 136 = two
+  // full waves 2606 Mbit/s, window 128 = 2.07 waves 2457 Mbit/s).
+  const int64_t wave = static_cast<int64_t>(sm_count_) * kMinBlocks * kThreads;
+  for (int j = 2; j <= 4; ++j) {
+    for (int w = std::max(guard, kGroup); w <= 1024; w += kGroup) {
+      int64_t windows = 0;
+      for (size_t i = 0; i < rq_in.n_cb; ++i) windows += (rq_in.cbs[i].k + w - 1) / w;
+      if (windows <= j * wave) {
+        bool have = false;
+        for (const Cand& c : cands) have |= !c.persistent && c.window == w;
+        if (!have) cands.push_back(Cand{false, w});
+        break;
+      }
+    }
+  }
   cudaStream_t st = static_cast<cudaStream_t>(rq_in.stream);
   cudaEvent_t a, b;
   check(cudaEventCreate(&a), "cudaEventCreate");
   check(cudaEventCreate(&b), "cudaEventCreate");
   TuneChoice best;
   best.ms = 1e30;
-  const int guard = rq_in.guard < 0 ? kDefaultGuard : rq_in.guard;
   try {
     for (const Cand& c : cands) {
       if (c.window < guard) continue;
