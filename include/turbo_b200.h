@@ -80,6 +80,25 @@ TC_API int tc_derate_match_bits(int32_t k, int32_t filler, const uint8_t* e_bits
 TC_API int tc_derate_match_llr(int32_t k, int32_t filler, const float* e_llr, size_t e, uint32_t rv,
                         float* d012_llr);
 
+/* ---------------- the TS 36.212 code (new; off by default) ----------------
+ * Everything above follows the reference's code, which departs from TS 36.212 in its
+ * constituent encoder (feedback g0 = 1+D+D^2 where 36.212 5.1.3.2.1 has 1+D^2+D^3;
+ * lte_turbo.cpp:333-341), its CRC generators (the coefficient arrays of lte_turbo.cpp:104-116
+ * instead of the 36.212 5.1.1 polynomials) and its trellis-termination multiplexing
+ * (lte_turbo.cpp:664-677 instead of 36.212 5.1.3.2.2).  TC_CONVENTION_3GPP selects the 36.212
+ * code in these functions and, through tc_decode_options.convention, in the decoders.  QPP
+ * interleaving, segmentation sizes, filler handling, the circular buffer and rate matching are
+ * common to both conventions (no limited-buffer rate matching in either).  The _conv functions
+ * with TC_CONVENTION_REFERENCE are the functions above. */
+enum { TC_CONVENTION_REFERENCE = 0, TC_CONVENTION_3GPP = 1 };
+TC_API int tc_crc_append_conv(int convention, int kind, const uint8_t* bits, size_t n,
+                              uint8_t* out /* n + L */);
+TC_API int tc_crc_check_conv(int convention, int kind, const uint8_t* bits, size_t n, int* ok);
+TC_API int tc_segment_transport_block_conv(int convention, const uint8_t* bits_with_crc, size_t b,
+                                           tc_segmentation* info, uint8_t* cb_bits, size_t cap);
+TC_API int tc_turbo_encode_conv(int convention, int32_t k, int32_t filler, const uint8_t* cb_bits,
+                                uint8_t* d012);
+
 /* ---------------- seeded test channel (new; used by tests and the benchmark) ---------------- */
 TC_API int tc_random_bits(uint64_t seed, uint64_t first, size_t n, uint8_t* bits);
 TC_API int tc_awgn_llr(uint64_t seed, uint64_t first, const uint8_t* bits, size_t n, double sigma2,
@@ -131,9 +150,17 @@ typedef struct {
   const float* scales;     /* host array, 2 per iteration (upper, lower); NULL = 1.0     */
   uint32_t graph;          /* TC_MEM_DEVICE only: capture this request's launch sequence in a
                               CUDA graph the first time and replay it when the same shapes,
-                              buffers and options come again (16 graphs kept per decoder)  */
+                              buffers and options come again (16 graphs kept per decoder);
+                              needs a created stream (the legacy default stream cannot be
+                              captured: TC_ERR_INVALID_ARGUMENT)                          */
   void* stream;            /* cudaStream_t; TC_MEM_DEVICE: used as given (NULL = the legacy
                               default stream); TC_MEM_HOST: NULL = the decoder's own stream */
+  uint32_t convention;     /* TC_CONVENTION_REFERENCE (default) or TC_CONVENTION_3GPP: the code
+                              the LLRs come from (trellis, tail multiplexing, CRC24B of the
+                              early stop; CRC24A too in tc_decode_transport_blocks).  Honoured
+                              by tc_decode (every schedule and memory kind), tc_autotune and
+                              tc_decode_transport_blocks; tc_decode_noalloc refuses the 3GPP
+                              code (TC_ERR_INVALID_ARGUMENT); the adjoint is the reference's */
 } tc_decode_options;
 
 TC_API int tc_decode_options_init(tc_decode_options* opts);

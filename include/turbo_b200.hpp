@@ -51,6 +51,8 @@ struct LteTurboCodecParams {
   std::size_t n_soft = 0;
   std::uint32_t max_iterations = 8;
   bool enable_early_stop = false;
+  // new: TC_CONVENTION_REFERENCE (the reference's code) or TC_CONVENTION_3GPP (TS 36.212)
+  std::uint32_t convention = TC_CONVENTION_REFERENCE;
 };
 
 struct CodeBlockDescriptor {
@@ -139,15 +141,15 @@ inline tc_decoder* decoder() {
 }
 
 inline std::vector<std::uint8_t> crc_append(int kind, std::span<const std::uint8_t> bits,
-                                            std::size_t len) {
+                                            std::size_t len, std::uint32_t conv) {
   std::vector<std::uint8_t> out(bits.size() + len);
-  check(tc_crc_append(kind, bits.data(), bits.size(), out.data()));
+  check(tc_crc_append_conv(static_cast<int>(conv), kind, bits.data(), bits.size(), out.data()));
   return out;
 }
 
-inline bool crc_check(int kind, std::span<const std::uint8_t> bits) {
+inline bool crc_check(int kind, std::span<const std::uint8_t> bits, std::uint32_t conv) {
   int ok = 0;
-  check(tc_crc_check(kind, bits.data(), bits.size(), &ok));
+  check(tc_crc_check_conv(static_cast<int>(conv), kind, bits.data(), bits.size(), &ok));
   return ok != 0;
 }
 
@@ -189,24 +191,27 @@ inline std::vector<std::size_t> qpp_inverse_permutation(std::size_t k) {
   return std::vector<std::size_t>(p.begin(), p.end());
 }
 
-// ---- CRC (lte_turbo.h:97-104) ----
-inline std::vector<std::uint8_t> append_crc24a(std::span<const std::uint8_t> b) { return detail::crc_append(TC_CRC24A, b, 24); }
-inline std::vector<std::uint8_t> append_crc24b(std::span<const std::uint8_t> b) { return detail::crc_append(TC_CRC24B, b, 24); }
-inline std::vector<std::uint8_t> append_crc16(std::span<const std::uint8_t> b) { return detail::crc_append(TC_CRC16, b, 16); }
-inline std::vector<std::uint8_t> append_crc8(std::span<const std::uint8_t> b) { return detail::crc_append(TC_CRC8, b, 8); }
-inline bool check_crc24a(std::span<const std::uint8_t> b) { return detail::crc_check(TC_CRC24A, b); }
-inline bool check_crc24b(std::span<const std::uint8_t> b) { return detail::crc_check(TC_CRC24B, b); }
-inline bool check_crc16(std::span<const std::uint8_t> b) { return detail::crc_check(TC_CRC16, b); }
-inline bool check_crc8(std::span<const std::uint8_t> b) { return detail::crc_check(TC_CRC8, b); }
+// ---- CRC (lte_turbo.h:97-104); conv (new): TC_CONVENTION_3GPP for the TS 36.212 generators ----
+constexpr std::uint32_t kRef = TC_CONVENTION_REFERENCE;
+inline std::vector<std::uint8_t> append_crc24a(std::span<const std::uint8_t> b, std::uint32_t conv = kRef) { return detail::crc_append(TC_CRC24A, b, 24, conv); }
+inline std::vector<std::uint8_t> append_crc24b(std::span<const std::uint8_t> b, std::uint32_t conv = kRef) { return detail::crc_append(TC_CRC24B, b, 24, conv); }
+inline std::vector<std::uint8_t> append_crc16(std::span<const std::uint8_t> b, std::uint32_t conv = kRef) { return detail::crc_append(TC_CRC16, b, 16, conv); }
+inline std::vector<std::uint8_t> append_crc8(std::span<const std::uint8_t> b, std::uint32_t conv = kRef) { return detail::crc_append(TC_CRC8, b, 8, conv); }
+inline bool check_crc24a(std::span<const std::uint8_t> b, std::uint32_t conv = kRef) { return detail::crc_check(TC_CRC24A, b, conv); }
+inline bool check_crc24b(std::span<const std::uint8_t> b, std::uint32_t conv = kRef) { return detail::crc_check(TC_CRC24B, b, conv); }
+inline bool check_crc16(std::span<const std::uint8_t> b, std::uint32_t conv = kRef) { return detail::crc_check(TC_CRC16, b, conv); }
+inline bool check_crc8(std::span<const std::uint8_t> b, std::uint32_t conv = kRef) { return detail::crc_check(TC_CRC8, b, conv); }
 
 // ---- segmentation (lte_turbo.h:106): the K- blocks first, then the K+ blocks ----
-inline SegmentationResult segment_transport_block(std::span<const std::uint8_t> bits_with_crc) {
+inline SegmentationResult segment_transport_block(std::span<const std::uint8_t> bits_with_crc,
+                                                  std::uint32_t conv = kRef) {
   tc_segmentation info{};
-  detail::check(tc_segment_transport_block(bits_with_crc.data(), bits_with_crc.size(), &info,
-                                           nullptr, 0));
+  const int c = static_cast<int>(conv);
+  detail::check(tc_segment_transport_block_conv(c, bits_with_crc.data(), bits_with_crc.size(),
+                                                &info, nullptr, 0));
   std::vector<std::uint8_t> all(info.c_plus * info.k_plus + info.c_minus * info.k_minus);
-  detail::check(tc_segment_transport_block(bits_with_crc.data(), bits_with_crc.size(), &info,
-                                           all.data(), all.size()));
+  detail::check(tc_segment_transport_block_conv(c, bits_with_crc.data(), bits_with_crc.size(),
+                                                &info, all.data(), all.size()));
   SegmentationResult out{info.c, info.c_plus, info.c_minus, info.k_plus, info.k_minus,
                          info.filler_bits, info.l, {}};
   std::size_t pos = 0;
@@ -220,16 +225,20 @@ inline SegmentationResult segment_transport_block(std::span<const std::uint8_t> 
 }
 
 // ---- encoder and rate matching (lte_turbo.h:111-118) ----
-// The tail bits: each encoder's termination input is s1^s2 (feedback 0), so its third input
-// is always 0 and its third parity equals its second input; the multiplexed streams (d0, d1,
-// d2 tails) carry the rest.
+// The tail bits, reference code: each encoder's termination input is s1^s2 (feedback 0), so its
+// third input is always 0 and its third parity equals its second input; the multiplexed streams
+// (d0, d1, d2 tails) carry the rest.  TS 36.212 code: the twelve tail bits are all in the
+// streams (5.1.3.2.2), x_K..x_K+2 = d0[K], d2[K], d1[K+1] and z_K..z_K+2 = d1[K], d0[K+1],
+// d2[K+1] for the upper encoder, the same two positions on for the lower one.
 inline EncodedCodeBlock turbo_encode_code_block(const CodeBlockDescriptor& descriptor,
-                                                std::span<const std::uint8_t> cb_bits) {
+                                                std::span<const std::uint8_t> cb_bits,
+                                                std::uint32_t conv = kRef) {
   if (cb_bits.size() != descriptor.k_r) throw std::invalid_argument("code block length mismatch");
   const std::size_t k = descriptor.k_r;
   std::vector<std::uint8_t> d(3 * (k + 4));
-  detail::check(tc_turbo_encode(static_cast<int32_t>(k), static_cast<int32_t>(descriptor.filler_count),
-                                cb_bits.data(), d.data()));
+  detail::check(tc_turbo_encode_conv(static_cast<int>(conv), static_cast<int32_t>(k),
+                                     static_cast<int32_t>(descriptor.filler_count), cb_bits.data(),
+                                     d.data()));
   EncodedCodeBlock out;
   out.descriptor = descriptor;
   out.descriptor.d_r = k + 4;
@@ -241,6 +250,13 @@ inline EncodedCodeBlock turbo_encode_code_block(const CodeBlockDescriptor& descr
   const std::uint8_t* d0 = d.data();
   const std::uint8_t* d1 = d0 + (k + 4);
   const std::uint8_t* d2 = d1 + (k + 4);
+  if (conv == TC_CONVENTION_3GPP) {
+    out.upper_tail_systematic = {d0[k], d2[k], d1[k + 1]};
+    out.upper_tail_parity = {d1[k], d0[k + 1], d2[k + 1]};
+    out.lower_tail_systematic = {d0[k + 2], d2[k + 2], d1[k + 3]};
+    out.lower_tail_parity = {d1[k + 2], d0[k + 3], d2[k + 3]};
+    return out;
+  }
   out.upper_tail_systematic = {d0[k], d0[k + 2], 0};
   out.upper_tail_parity = {d1[k], d0[k + 1], d0[k + 3]};
   out.lower_tail_systematic = {d1[k + 3], d2[k + 1], d2[k + 3]};
@@ -255,8 +271,8 @@ inline EncodedTransportBlock encode_transport_block(const LteTurboCodecParams& p
   EncodedTransportBlock out;
   out.params = params;
   out.transport_bits.assign(transport_bits.begin(), transport_bits.end());
-  out.tb_bits_with_crc = append_crc24a(transport_bits);
-  const SegmentationResult seg = segment_transport_block(out.tb_bits_with_crc);
+  out.tb_bits_with_crc = append_crc24a(transport_bits, params.convention);
+  const SegmentationResult seg = segment_transport_block(out.tb_bits_with_crc, params.convention);
   for (std::size_t r = 0; r < seg.code_blocks.size(); ++r) {
     const auto& bits = seg.code_blocks[r];
     CodeBlockDescriptor desc;
@@ -269,7 +285,7 @@ inline EncodedTransportBlock encode_transport_block(const LteTurboCodecParams& p
     int32_t qi = 0;
     detail::check(tc_qpp_index(static_cast<int32_t>(desc.k_r), &qi));
     desc.qpp_index = static_cast<std::size_t>(qi);
-    EncodedCodeBlock enc = turbo_encode_code_block(desc, bits);
+    EncodedCodeBlock enc = turbo_encode_code_block(desc, bits, params.convention);
     std::vector<std::uint8_t> d012(enc.systematic);
     d012.insert(d012.end(), enc.parity0.begin(), enc.parity0.end());
     d012.insert(d012.end(), enc.parity1.begin(), enc.parity1.end());
@@ -302,7 +318,8 @@ inline std::vector<float> decode_code_blocks(std::span<const std::size_t> ks,
                                              std::uint32_t max_iterations, bool enable_early_stop,
                                              DecoderBackend backend,
                                              std::vector<bool>* crc_ok = nullptr,
-                                             std::vector<std::uint32_t>* iterations_used = nullptr) {
+                                             std::vector<std::uint32_t>* iterations_used = nullptr,
+                                             std::uint32_t conv = kRef) {
   if (backend == DecoderBackend::CpuReference)
     throw std::invalid_argument("CPU decoding is not part of turbo_b200; use a GPU backend");
   if (fillers.size() != ks.size()) throw std::invalid_argument("one filler count per block");
@@ -322,6 +339,7 @@ inline std::vector<float> decode_code_blocks(std::span<const std::size_t> ks,
   o.window = backend == DecoderBackend::GpuStage1Exact ? 6144 : 0;
   o.schedule = backend == DecoderBackend::GpuB200Persistent ? TC_SCHEDULE_PERSISTENT
                                                             : TC_SCHEDULE_PLAIN;
+  o.convention = conv;
   std::vector<float> post(static_cast<std::size_t>(po));
   std::vector<std::uint8_t> ok(ks.size());
   std::vector<std::uint32_t> used(ks.size());
@@ -398,7 +416,7 @@ inline DecodedTransportBlock decode_transport_block(const LteTurboCodecParams& p
   DecodedTransportBlock out;
   out.posterior_llr =
       decode_code_blocks(ks, fillers, llr, params.max_iterations, params.enable_early_stop,
-                         backend, nullptr, &used);
+                         backend, nullptr, &used, params.convention);
   std::vector<std::uint8_t> tb;
   std::size_t pos = 0;
   for (std::size_t i = 0; i < ks.size(); ++i) {
@@ -409,13 +427,13 @@ inline DecodedTransportBlock decode_transport_block(const LteTurboCodecParams& p
     pos += ks[i];
     bool ok = true;
     if (ks.size() > 1) {
-      ok = check_crc24b(hard);
+      ok = check_crc24b(hard, params.convention);
       hard.resize(hard.size() - 24);
     }
     tb.insert(tb.end(), hard.begin(), hard.end());
     out.code_block_crc_ok.push_back(ok);
   }
-  out.transport_block_crc_ok = check_crc24a(tb);
+  out.transport_block_crc_ok = check_crc24a(tb, params.convention);
   out.tb_bits.assign(tb.begin(), tb.end() - 24);
   return out;
 }

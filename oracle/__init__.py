@@ -80,6 +80,12 @@ class Oracle(_Lib):
         _sig(L, "or_decode_batch", None, batch_args + [_i32p, _i32p, C.c_int32])
         _sig(L, "or_decode_batch_windowed", None,
              batch_args + [C.c_int32, C.c_int32, _i32p, _i32p, C.c_int32])
+        _sig(L, "or_std_crc_append", None, [C.c_int, _u8p, C.c_size_t, _u8p])
+        _sig(L, "or_std_crc_check", C.c_int, [C.c_int, _u8p, C.c_size_t])
+        _sig(L, "or_std_turbo_encode", None, [C.c_int32, C.c_int32, _u8p, _u8p, _u8p, _u8p])
+        _sig(L, "or_std_decode_cb_windowed", None,
+             [C.c_int32, C.c_int32, _f32p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _f32p,
+              C.POINTER(C.c_int32), C.POINTER(C.c_int32)])
         _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
         _f64n = C.POINTER(C.c_double)
         _sig(L, "or_adj_seed_count", C.c_int64, [C.c_int32, C.c_int32, C.c_int32])
@@ -166,6 +172,32 @@ class Oracle(_Lib):
         else:
             self.lib.or_decode_cb(k, filler, llr, iters, int(early_stop), post, C.byref(ok),
                                   C.byref(used))
+        return post, bool(ok.value), used.value
+
+    # -- the TS 36.212 code (no reference counterpart) --
+    def std_crc_append(self, kind: int, bits) -> np.ndarray:
+        b = np.ascontiguousarray(bits, np.uint8)
+        out = np.empty(b.size + CRC_LEN[kind], np.uint8)
+        self.lib.or_std_crc_append(kind, b, b.size, out)
+        return out
+
+    def std_crc_check(self, kind: int, bits) -> bool:
+        b = np.ascontiguousarray(bits, np.uint8)
+        return bool(self.lib.or_std_crc_check(kind, b, b.size))
+
+    def std_turbo_encode(self, k: int, filler: int, cb) -> np.ndarray:
+        cbb = np.ascontiguousarray(cb, np.uint8)
+        d = [np.empty(k + 4, np.uint8) for _ in range(3)]
+        self.lib.or_std_turbo_encode(k, filler, cbb, *d)
+        return np.concatenate(d)
+
+    def std_decode_cb(self, k, filler, llr, iters=8, early_stop=False, window=0, guard=0):
+        """The windowed schedule (window 0: full trellis) on the TS 36.212 code."""
+        llr = np.ascontiguousarray(llr, np.float32)
+        post = np.empty(k, np.float32)
+        ok, used = C.c_int32(), C.c_int32()
+        self.lib.or_std_decode_cb_windowed(k, filler, llr, iters, int(early_stop), window, guard,
+                                           post, C.byref(ok), C.byref(used))
         return post, bool(ok.value), used.value
 
     # -- FP64 differentiable decoder (scaled extrinsics, windowed schedule) and its adjoint --

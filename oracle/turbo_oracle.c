@@ -105,10 +105,55 @@ int or_crc_len(int kind) {
   return len;
 }
 
-/* lte_turbo.cpp:118-135 */
+/* TS 36.212 5.1.1 generator polynomials, written the same way (no reference counterpart):
+ * gCRC24A = D^24+D^23+D^18+D^17+D^14+D^11+D^10+D^7+D^6+D^5+D^4+D^3+D+1,
+ * gCRC24B = D^24+D^23+D^6+D^5+D+1, gCRC16 = D^16+D^12+D^5+1, gCRC8 = D^8+D^7+D^4+D^3+D+1 */
+static const uint8_t kS24A[24] = {1, 0, 0, 0, 0, 1, 1, 0, 0, 1, 0, 0,
+                                  1, 1, 0, 0, 1, 1, 1, 1, 1, 0, 1, 1};
+static const uint8_t kS24B[24] = {1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,
+                                  0, 0, 0, 0, 0, 1, 1, 0, 0, 0, 1, 1};
+static const uint8_t kS16[16] = {0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+static const uint8_t kS8[8] = {1, 0, 0, 1, 1, 0, 1, 1};
+
+static const uint8_t* crc_poly_conv(int conv, int kind, int* len) {
+  if (!conv) return crc_poly(kind, len);
+  switch (kind) {
+    case 0: *len = 24; return kS24A;
+    case 1: *len = 24; return kS24B;
+    case 2: *len = 16; return kS16;
+    default: *len = 8; return kS8;
+  }
+}
+
+static void crc_append_g(const uint8_t* g, int len, const uint8_t* bits, size_t n, uint8_t* out);
+static int crc_check_g(const uint8_t* g, int len, const uint8_t* bits, size_t n);
+
 void or_crc_append(int kind, const uint8_t* bits, size_t n, uint8_t* out) {
   int len;
   const uint8_t* g = crc_poly(kind, &len);
+  crc_append_g(g, len, bits, n, out);
+}
+
+int or_crc_check(int kind, const uint8_t* bits, size_t n) {
+  int len;
+  const uint8_t* g = crc_poly(kind, &len);
+  return crc_check_g(g, len, bits, n);
+}
+
+void or_std_crc_append(int kind, const uint8_t* bits, size_t n, uint8_t* out) {
+  int len;
+  const uint8_t* g = crc_poly_conv(1, kind, &len);
+  crc_append_g(g, len, bits, n, out);
+}
+
+int or_std_crc_check(int kind, const uint8_t* bits, size_t n) {
+  int len;
+  const uint8_t* g = crc_poly_conv(1, kind, &len);
+  return crc_check_g(g, len, bits, n);
+}
+
+/* lte_turbo.cpp:118-135 */
+static void crc_append_g(const uint8_t* g, int len, const uint8_t* bits, size_t n, uint8_t* out) {
   uint8_t* work = (uint8_t*)calloc(n + (size_t)len, 1);
   memcpy(work, bits, n);
   for (size_t i = 0; i < n; ++i) {
@@ -122,9 +167,7 @@ void or_crc_append(int kind, const uint8_t* bits, size_t n, uint8_t* out) {
 }
 
 /* lte_turbo.cpp:137-155: divide all but the last L bits; remainder must be zero. */
-int or_crc_check(int kind, const uint8_t* bits, size_t n) {
-  int len;
-  const uint8_t* g = crc_poly(kind, &len);
+static int crc_check_g(const uint8_t* g, int len, const uint8_t* bits, size_t n) {
   if (n < (size_t)len) return 0;
   uint8_t* work = (uint8_t*)malloc(n ? n : 1);
   memcpy(work, bits, n);
@@ -214,6 +257,49 @@ static void termination(uint8_t state, uint8_t in[3]) {
     in[i] = u;
     rsc_step(state, u, &p, &state);
   }
+}
+
+/* TS 36.212 5.1.3.2.1 (no reference counterpart): transfer function [1, g1(D)/g0(D)],
+ * g0 = 1 + D^2 + D^3, g1 = 1 + D + D^3.  The register holds r1 (delay D), r2 (D^2), r3 (D^3);
+ * state = r1 | r2 << 1 | r3 << 2, a labelling of this file's own. */
+static void rsc_step_std(uint8_t state, uint8_t u, uint8_t* parity, uint8_t* next) {
+  const uint8_t r1 = state & 1u, r2 = (state >> 1) & 1u, r3 = (state >> 2) & 1u;
+  const uint8_t a = u ^ r2 ^ r3; /* register input: g0 taps D^2, D^3 fed back */
+  *parity = a ^ r1 ^ r3;         /* g1 taps 1, D, D^3 */
+  *next = (uint8_t)(a | (r1 << 1) | (r2 << 2));
+}
+
+/* 5.1.3.2.2: with the switch in the lower position the input is the feedback r2^r3, so the
+ * register input is 0; the systematic tail bit is that input. */
+static uint8_t term_input_std(uint8_t state) { return ((state >> 1) & 1u) ^ ((state >> 2) & 1u); }
+
+void or_std_turbo_encode(int32_t k, int32_t filler, const uint8_t* cb, uint8_t* d0, uint8_t* d1,
+                         uint8_t* d2) {
+  int32_t* perm = (int32_t*)malloc(sizeof(int32_t) * (size_t)k);
+  or_qpp_perm(k, perm);
+  uint8_t su = 0, sl = 0, p, n;
+  for (int32_t i = 0; i < k; ++i) { /* 5.1.3.2.1, filler bits as <NULL> in d0 and d1 */
+    rsc_step_std(su, cb[i], &p, &n);
+    su = n;
+    d0[i] = (i < filler) ? 0 : cb[i];
+    d1[i] = (i < filler) ? 0 : p;
+    rsc_step_std(sl, cb[perm[i]], &p, &n);
+    sl = n;
+    d2[i] = p;
+  }
+  uint8_t x[3], z[3], xp[3], zp[3]; /* x_K+i, z_K+i, x'_K+i, z'_K+i */
+  for (int i = 0; i < 3; ++i) {
+    x[i] = term_input_std(su);
+    rsc_step_std(su, x[i], &z[i], &su);
+    xp[i] = term_input_std(sl);
+    rsc_step_std(sl, xp[i], &zp[i], &sl);
+  }
+  /* 5.1.3.2.2: d0 = x_K z_K+1 x'_K z'_K+1, d1 = z_K x_K+2 z'_K x'_K+2,
+   * d2 = x_K+1 z_K+2 x'_K+1 z'_K+2 */
+  d0[k + 0] = x[0]; d0[k + 1] = z[1]; d0[k + 2] = xp[0]; d0[k + 3] = zp[1];
+  d1[k + 0] = z[0]; d1[k + 1] = x[2]; d1[k + 2] = zp[0]; d1[k + 3] = xp[2];
+  d2[k + 0] = x[1]; d2[k + 1] = z[2]; d2[k + 2] = xp[1]; d2[k + 3] = zp[2];
+  free(perm);
 }
 
 /* lte_turbo.cpp:624-688 */
@@ -382,14 +468,26 @@ void or_derate_llr(int32_t d, int32_t filler, const float* e_llr, size_t e, int3
 /* ------------------------------------------------------------------------------------------ */
 typedef struct {
   uint8_t parity[8][2], next[8][2];
+  uint8_t term[8]; /* the input that zeroes the register input (trellis termination) */
+  int std;         /* 1: the TS 36.212 code (tail mapping and CRC too) */
 } trellis_t;
 
-static trellis_t make_trellis(void) {
+static trellis_t make_trellis_conv(int std) {
   trellis_t t;
-  for (int s = 0; s < 8; ++s)
-    for (int u = 0; u < 2; ++u) rsc_step((uint8_t)s, (uint8_t)u, &t.parity[s][u], &t.next[s][u]);
+  t.std = std;
+  for (int s = 0; s < 8; ++s) {
+    for (int u = 0; u < 2; ++u) {
+      if (std) rsc_step_std((uint8_t)s, (uint8_t)u, &t.parity[s][u], &t.next[s][u]);
+      else rsc_step((uint8_t)s, (uint8_t)u, &t.parity[s][u], &t.next[s][u]);
+    }
+    uint8_t in[3];
+    termination((uint8_t)s, in);
+    t.term[s] = std ? term_input_std((uint8_t)s) : in[0];
+  }
   return t;
 }
+
+static trellis_t make_trellis(void) { return make_trellis_conv(0); }
 
 /* lte_turbo.cpp:380-390 */
 static float max_star(float x, float y) {
@@ -411,16 +509,14 @@ static void normalize8(float* m) {
 }
 
 /* lte_turbo.cpp:357-378 */
-static void tail_beta(const float ts[4], const float tp[4], float beta[8]) {
+static void tail_beta(const trellis_t* T, const float ts[4], const float tp[4], float beta[8]) {
   for (int s = 0; s < 8; ++s) {
-    uint8_t cur = (uint8_t)s, in[3];
+    uint8_t cur = (uint8_t)s;
     float metric = 0.0f;
-    termination(cur, in);
     for (int i = 0; i < 3; ++i) {
-      uint8_t p, n;
-      rsc_step(cur, in[i], &p, &n);
-      cur = n;
-      const float sys_term = 0.5f * ((in[i] ? 1.0f : -1.0f) * ts[i]);
+      const uint8_t in = T->term[cur], p = T->parity[cur][in];
+      cur = T->next[cur][in];
+      const float sys_term = 0.5f * ((in ? 1.0f : -1.0f) * ts[i]);
       const float par_term = 0.5f * ((p ? 1.0f : -1.0f) * tp[i]);
       metric += sys_term + par_term;
     }
@@ -513,12 +609,24 @@ static void gather_tails(int32_t k, const float* d0, const float* d1, const floa
   ltp[0] = d2[k + 1]; ltp[1] = d0[k + 3]; ltp[2] = d2[k + 3]; ltp[3] = 0.0f;
 }
 
+/* The tail LLRs of the TS 36.212 multiplexing (5.1.3.2.2; no reference counterpart):
+ * upper systematic x_K..x_K+2 = d0[K], d2[K], d1[K+1], parity z_K..z_K+2 = d1[K], d0[K+1],
+ * d2[K+1]; lower x'_K.. = d0[K+2], d2[K+2], d1[K+3], z'_K.. = d1[K+2], d0[K+3], d2[K+3]. */
+static void gather_tails_std(int32_t k, const float* d0, const float* d1, const float* d2,
+                             float uts[4], float utp[4], float lts[4], float ltp[4]) {
+  uts[0] = d0[k + 0]; uts[1] = d2[k + 0]; uts[2] = d1[k + 1]; uts[3] = 0.0f;
+  utp[0] = d1[k + 0]; utp[1] = d0[k + 1]; utp[2] = d2[k + 1]; utp[3] = 0.0f;
+  lts[0] = d0[k + 2]; lts[1] = d2[k + 2]; lts[2] = d1[k + 3]; lts[3] = 0.0f;
+  ltp[0] = d1[k + 2]; ltp[1] = d0[k + 3]; ltp[2] = d2[k + 3]; ltp[3] = 0.0f;
+}
+
 /* hard decision >= 0 -> 1, zero the filler, CRC24B over the rest (lte_turbo.cpp:488-494,
  * 792-797) */
-static int early_stop_crc(const float* post, int32_t k, int32_t filler, uint8_t* hard) {
+static int early_stop_crc(const float* post, int32_t k, int32_t filler, uint8_t* hard, int std) {
   for (int32_t i = 0; i < k; ++i) hard[i] = post[i] >= 0.0f ? 1u : 0u;
   for (int32_t i = 0; i < filler; ++i) hard[i] = 0;
-  return or_crc_check(1, hard + filler, (size_t)(k - filler));
+  return std ? or_std_crc_check(1, hard + filler, (size_t)(k - filler))
+             : or_crc_check(1, hard + filler, (size_t)(k - filler));
 }
 
 /*
@@ -532,8 +640,8 @@ static int early_stop_crc(const float* post, int32_t k, int32_t filler, uint8_t*
  */
 static void decode_common(int32_t k, int32_t filler, const float* llr, int32_t max_iterations,
                           int32_t early_stop, int32_t window, int32_t guard, float* posterior,
-                          int32_t* crc_ok, int32_t* iterations_used) {
-  const trellis_t T = make_trellis();
+                          int32_t* crc_ok, int32_t* iterations_used, int std) {
+  const trellis_t T = make_trellis_conv(std);
   const float* d0 = llr;
   const float* d1 = llr + (k + 4);
   const float* d2 = llr + 2 * (k + 4);
@@ -562,10 +670,11 @@ static void decode_common(int32_t k, int32_t filler, const float* llr, int32_t m
   for (int32_t i = 0; i < k; ++i) sys_i[i] = d0[perm[i]];
 
   float tails[4][4];
-  gather_tails(k, d0, d1, d2, tails[0], tails[1], tails[2], tails[3]);
+  if (std) gather_tails_std(k, d0, d1, d2, tails[0], tails[1], tails[2], tails[3]);
+  else gather_tails(k, d0, d1, d2, tails[0], tails[1], tails[2], tails[3]);
   float tb[2][8];
-  tail_beta(tails[0], tails[1], tb[0]);
-  tail_beta(tails[2], tails[3], tb[1]);
+  tail_beta(&T, tails[0], tails[1], tb[0]);
+  tail_beta(&T, tails[2], tails[3], tb[1]);
   float a_start[8];
   for (int s = 0; s < 8; ++s) a_start[s] = s == 0 ? 0.0f : -INFINITY;
 
@@ -606,7 +715,7 @@ static void decode_common(int32_t k, int32_t filler, const float* llr, int32_t m
     }
     if (iterations_used) *iterations_used = it + 1;
     if (early_stop) {
-      ok = early_stop_crc(posterior, k, filler, hard);
+      ok = early_stop_crc(posterior, k, filler, hard, std);
       if (ok) break;
     }
   }
@@ -620,7 +729,7 @@ void or_decode_cb(int32_t k, int32_t filler, const float* llr, int32_t max_itera
                   int32_t* iterations_used) {
   if (iterations_used) *iterations_used = 0;
   decode_common(k, filler, llr, max_iterations, early_stop, 0, 0, posterior, crc_ok,
-                iterations_used);
+                iterations_used, 0);
 }
 
 void or_decode_cb_windowed(int32_t k, int32_t filler, const float* llr, int32_t max_iterations,
@@ -628,7 +737,17 @@ void or_decode_cb_windowed(int32_t k, int32_t filler, const float* llr, int32_t 
                            int32_t* crc_ok, int32_t* iterations_used) {
   if (iterations_used) *iterations_used = 0;
   decode_common(k, filler, llr, max_iterations, early_stop, window, guard, posterior, crc_ok,
-                iterations_used);
+                iterations_used, 0);
+}
+
+/* The same schedule on the TS 36.212 code (trellis, tail mapping, CRC24B of the early stop). */
+void or_std_decode_cb_windowed(int32_t k, int32_t filler, const float* llr,
+                               int32_t max_iterations, int32_t early_stop, int32_t window,
+                               int32_t guard, float* posterior, int32_t* crc_ok,
+                               int32_t* iterations_used) {
+  if (iterations_used) *iterations_used = 0;
+  decode_common(k, filler, llr, max_iterations, early_stop, window, guard, posterior, crc_ok,
+                iterations_used, 1);
 }
 
 /* ------------------------------------------------------------------------------------------ */
@@ -655,8 +774,7 @@ static void* batch_worker(void* p) {
     if (i >= b->n) break;
     int32_t c = 0, u = 0;
     decode_common(b->k[i], b->filler[i], b->llr + b->llr_off[i], b->iters, b->early, b->window,
-                  b->guard,
-                  b->post + b->out_off[i], &c, &u);
+                  b->guard, b->post + b->out_off[i], &c, &u, 0);
     if (b->crc) b->crc[i] = c;
     if (b->used) b->used[i] = u;
   }

@@ -106,6 +106,19 @@ void or_adj_vjp(int32_t k, const double* llr, int32_t iters, const double* scale
                 const double* grad_post, double* posterior, double* grad_llr,
                 double* grad_scales, double* seeds_out);
 
+/* ---- the TS 36.212 code (no reference counterpart; restated from 36.212 5.1.1 and
+ * 5.1.3.2): CRC generator polynomials, constituent encoder g0 = 1+D^2+D^3 / g1 = 1+D+D^3, trellis
+ * termination and tail multiplexing, and the windowed decoder above on that code.  Pinned by
+ * the published CRC check values and by encode/decode round trips, not by the reference. ---- */
+void or_std_crc_append(int kind, const uint8_t* bits, size_t n, uint8_t* out /* n + len */);
+int or_std_crc_check(int kind, const uint8_t* bits, size_t n);
+void or_std_turbo_encode(int32_t k, int32_t filler, const uint8_t* cb, uint8_t* d0, uint8_t* d1,
+                         uint8_t* d2);
+void or_std_decode_cb_windowed(int32_t k, int32_t filler, const float* llr,
+                               int32_t max_iterations, int32_t early_stop, int32_t window,
+                               int32_t guard, float* posterior, int32_t* crc_ok,
+                               int32_t* iterations_used);
+
 #ifdef __cplusplus
 }
 #endif

@@ -78,6 +78,20 @@ def awgn_blocks(tc, ks, ebn0_db, seed, fillers=None, crc24b=False):
     return llr, out
 
 
+def schedule_window(k, persistent):
+    """The window each schedule cuts block size k into (guard 96): plain 128 steps; persistent
+    at most 32 windows of at least 192 steps, of equal length rounded up to 8 (decoder.cu,
+    decode_persistent)."""
+    if not persistent:
+        return min(128, k)
+    nwin = max(1, min(32, k // 192))
+    wlen = -(-(-(-k // nwin)) // 8) * 8
+    if nwin > 1 and wlen < 96:
+        nwin = max(1, k // 96)
+        wlen = -(-(-(-k // nwin)) // 8) * 8
+    return min(wlen, k)
+
+
 def wilson(k: int, n: int, z: float = 1.96):
     """95% Wilson score interval of a binomial proportion k/n."""
     if n == 0:

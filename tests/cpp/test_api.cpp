@@ -10,6 +10,7 @@
 // check the encoder's tail arrays.
 #include <dlfcn.h>
 
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -24,6 +25,10 @@
 extern "C" void or_decode_cb(int32_t k, int32_t filler, const float* llr, int32_t max_iterations,
                              int32_t early_stop, float* posterior, int32_t* crc_ok,
                              int32_t* iterations_used);
+extern "C" void or_std_decode_cb_windowed(int32_t k, int32_t filler, const float* llr,
+                                          int32_t max_iterations, int32_t early_stop,
+                                          int32_t window, int32_t guard, float* posterior,
+                                          int32_t* crc_ok, int32_t* iterations_used);
 
 namespace tb = turbo_b200;
 
@@ -149,6 +154,55 @@ void encoder_cases(const char* ref_lib) {
   expect(tb::to_string(tb::LteChannelType::DL_SCH) == "DL_SCH", "channel type name");
 }
 
+// The TS 36.212 code (TC_CONVENTION_3GPP, an addition of this API): the published check values
+// of the 36.212 CRCs on ASCII "123456789", and the encoder's tail arrays against a constituent
+// encoder written here from g0 = 1 + D^2 + D^3, g1 = 1 + D + D^3.
+void std3gpp_codec_cases() {
+  std::vector<std::uint8_t> msg;
+  for (char ch : std::string("123456789"))
+    for (int b = 7; b >= 0; --b) msg.push_back(static_cast<std::uint8_t>((ch >> b) & 1));
+  const auto last = [](const std::vector<std::uint8_t>& v, std::size_t n) {
+    std::uint32_t r = 0;
+    for (std::size_t i = v.size() - n; i < v.size(); ++i) r = (r << 1) | v[i];
+    return r;
+  };
+  const std::uint32_t c3 = TC_CONVENTION_3GPP;
+  expect(last(tb::append_crc24a(msg, c3), 24) == 0xCDE703u, "36.212 CRC24A check value");
+  expect(last(tb::append_crc24b(msg, c3), 24) == 0x23EF52u, "36.212 CRC24B check value");
+  expect(last(tb::append_crc16(msg, c3), 16) == 0x31C3u, "36.212 CRC16 check value");
+  expect(last(tb::append_crc8(msg, c3), 8) == 0xEAu, "36.212 CRC8 check value");
+  expect(tb::check_crc24a(tb::append_crc24a(msg, c3), c3) && !tb::check_crc24a(tb::append_crc24a(msg, c3)),
+         "36.212 CRC24A is not the reference's");
+  for (std::size_t k : {40u, 1056u, 6144u}) {
+    const auto bits = pattern(k, 13, 1);
+    tb::CodeBlockDescriptor d;
+    d.k_r = k;
+    const auto enc = tb::turbo_encode_code_block(d, bits, c3);
+    const auto perm = tb::qpp_permutation(k);
+    for (int lower = 0; lower < 2; ++lower) {
+      int r1 = 0, r2 = 0, r3 = 0;  // delayed by D, D^2, D^3
+      bool parity_ok = true;
+      for (std::size_t i = 0; i < k; ++i) {
+        const int u = lower ? bits[perm[i]] : bits[i];
+        const int a = u ^ r2 ^ r3;
+        const int z = a ^ r1 ^ r3;
+        parity_ok &= z == (lower ? enc.parity1[i] : enc.parity0[i]);
+        r3 = r2; r2 = r1; r1 = a;
+      }
+      std::array<std::uint8_t, 3> xs{}, zs{};
+      for (int t = 0; t < 3; ++t) {
+        xs[t] = static_cast<std::uint8_t>(r2 ^ r3);
+        zs[t] = static_cast<std::uint8_t>(r1 ^ r3);  // register input 0
+        r3 = r2; r2 = r1; r1 = 0;
+      }
+      const std::string tag = "36.212 encoder K=" + std::to_string(k) + (lower ? " lower" : " upper");
+      expect(parity_ok, tag + ": parity");
+      expect(xs == (lower ? enc.lower_tail_systematic : enc.upper_tail_systematic), tag + ": tail x");
+      expect(zs == (lower ? enc.lower_tail_parity : enc.upper_tail_parity), tag + ": tail z");
+    }
+  }
+}
+
 double rel_err(const std::vector<float>& got, const std::vector<float>& ref) {
   double worst = 0.0;
   for (std::size_t i = 0; i < ref.size(); ++i)
@@ -209,7 +263,44 @@ void roundtrip_case(std::size_t tbs, std::size_t a, std::size_t c, bool g_from_b
   expect(hard && it == 6, "tile8 hard decisions");
 }
 
+// A transport block of the 36.212 code through the GPU backends, judged by the oracle's 36.212
+// restatement on the full trellis.
+void std3gpp_roundtrip_case(std::size_t tbs) {
+  tb::LteTurboCodecParams p;
+  p.transport_block_bits = tbs;
+  p.max_iterations = 6;
+  p.convention = TC_CONVENTION_3GPP;
+  const auto bits = pattern(tbs, 23, 7);
+  p.g_total = 0;
+  for (const auto& b :
+       tb::segment_transport_block(tb::append_crc24a(bits, p.convention), p.convention).code_blocks)
+    p.g_total += 3 * (b.size() + 4);
+  const auto enc = tb::encode_transport_block(p, bits);
+  std::vector<float> cpu;
+  for (const auto& b : enc.code_blocks) {
+    const auto llr = tb::derate_match_code_block(p, b.descriptor, b.rate_matched_bits);
+    std::vector<float> post(b.descriptor.k_r);
+    int32_t ok = 0, it = 0;
+    or_std_decode_cb_windowed(static_cast<int32_t>(b.descriptor.k_r),
+                              static_cast<int32_t>(b.descriptor.filler_count), llr.data(), 6, 0, 0,
+                              0, post.data(), &ok, &it);
+    cpu.insert(cpu.end(), post.begin(), post.end());
+  }
+  for (auto be : {tb::DecoderBackend::GpuStage1Exact, tb::DecoderBackend::GpuB200Persistent}) {
+    const auto dec = tb::decode_transport_block(p, enc, be);
+    const std::string tag = "36.212 TBS " + std::to_string(tbs) + " backend " + std::to_string(int(be));
+    expect(dec.tb_bits == bits && dec.transport_block_crc_ok, tag + ": round trip");
+    for (bool ok : dec.code_block_crc_ok) expect(ok, tag + ": code block CRC");
+    if (be == tb::DecoderBackend::GpuStage1Exact) {
+      const double err = rel_err(*dec.posterior_llr, cpu);
+      expect(err <= 1e-3, tag + ": posterior vs the oracle " + std::to_string(err));
+    }
+  }
+}
+
 void decoder_cases() {
+  std3gpp_roundtrip_case(1000);
+  std3gpp_roundtrip_case(12000);
   roundtrip_case(40, 7, 3, false, 3 * (64 + 4));
   roundtrip_case(512, 11, 5, false, 3 * (536 + 4));
   roundtrip_case(6112, 19, 11, true, 0);
@@ -237,6 +328,7 @@ int main(int argc, char** argv) {
     qpp_cases();
     segmentation_cases();
     encoder_cases(argc > 2 ? argv[2] : nullptr);
+    std3gpp_codec_cases();
     if (mode == "gpu") decoder_cases();
     std::printf("All %d checks passed (%s)\n", g_checks, mode.c_str());
     return 0;

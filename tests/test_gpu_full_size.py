@@ -17,7 +17,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import llr_close
+from conftest import llr_close, schedule_window
 
 pytestmark = pytest.mark.gpu
 
@@ -75,27 +75,13 @@ def test_config5_full_size(tc, decoder, oracle):
         sample = list(np.flatnonzero(ok == 0)[:5]) + list(np.flatnonzero(ok == 1)[:5]) + [0, 19999]
         for i in sample:
             k = int(ks[i])
+            win = schedule_window(k, sched == tc.SCHEDULE_PERSISTENT)
             ref, rok, rused = oracle.decode_cb(k, 0, llr[llr_off[i]:llr_off[i + 1]], 8, True,
-                                               window=_window(k, sched == tc.SCHEDULE_PERSISTENT),
-                                               guard=96)
+                                               window=win, guard=96)
             assert (bool(ok[i]), int(used[i])) == (rok, rused), (sched, i)
             err, hard = llr_close(post[starts[i]:starts[i] + k], ref)
             assert err <= 1e-3 and hard == 0, (sched, i, err)
     assert abs(pass_rate[0] - pass_rate[1]) <= 0.01, pass_rate
-
-
-def _window(k, persistent):
-    """The window each schedule cuts block size k into (guard 96): plain 128 steps; persistent
-    at most 32 windows of at least 192 steps, of equal length rounded up to 8 (decoder.cu,
-    decode_persistent)."""
-    if not persistent:
-        return min(128, k)
-    nwin = max(1, min(32, k // 192))
-    wlen = -(-(-(-k // nwin)) // 8) * 8
-    if nwin > 1 and wlen < 96:
-        nwin = max(1, k // 96)
-        wlen = -(-(-(-k // nwin)) // 8) * 8
-    return min(wlen, k)
 
 
 def test_config4_gradient_is_additive_over_sub_batches(tc, decoder):

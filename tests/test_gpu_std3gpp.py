@@ -1,0 +1,181 @@
+"""The TS 36.212 code on the GPU (DecodeOptions.convention = CONVENTION_3GPP; off by default).
+
+The decoder's other trellis, tail mapping and CRC24B are checked against the oracle's
+restatement of 36.212 running the same windows (flags and iterations equal, posteriors within
+1e-3), on both schedules; then the convention is shown to select the code (graph cache kept
+apart, LLRs of one code fail the other's CRC), and transport blocks of the 36.212 code make
+the round trip through the device chain with the 36.212 CRC24A/CRC24B.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import llr_close, schedule_window
+
+pytestmark = pytest.mark.gpu
+
+KS = [40, 48, 512, 1056, 2048, 4096, 6144, 6144, 1024, 3200]
+FILLERS = [0, 0, 0, 0, 0, 0, 0, 32, 16, 0]
+
+
+def std_code_blocks(tc, ks, ebn0_db, seed, fillers=None):
+    """BPSK/AWGN LLRs of 36.212 code blocks (K - 24 - F random bits + 36.212 CRC24B after F
+    filler zeros; filler LLRs zeroed).  Returns (LLRs back to back, code-block bits)."""
+    llrs, cbs = [], []
+    for i, k in enumerate(ks):
+        f = 0 if fillers is None else int(fillers[i])
+        data = tc.random_bits(seed * 1009 + i, k - 24 - f)
+        cb = np.concatenate([np.zeros(f, np.uint8), tc.append_crc24b(data, tc.CONVENTION_3GPP)])
+        desc = tc.CodeBlockDescriptor(0, k, k + 4, 0, f, tc.qpp_index(k))
+        e = tc.turbo_encode_code_block(desc, cb, tc.CONVENTION_3GPP)
+        d = np.concatenate([e.systematic, e.parity0, e.parity1])
+        sigma2 = 1.0 / (2.0 * (k / (3.0 * (k + 4))) * 10 ** (ebn0_db / 10.0))
+        x = tc.awgn_llr(seed * 7919 + i, d, sigma2)
+        x[:f] = 0.0
+        x[k + 4:k + 4 + f] = 0.0
+        llrs.append(x)
+        cbs.append(cb)
+    return np.concatenate(llrs), cbs
+
+
+@pytest.mark.parametrize("persistent", [False, True])
+def test_std_decode_matches_oracle(tc, decoder, oracle, persistent):
+    llr, _ = std_code_blocks(tc, KS, 0.7, seed=3)
+    sched = tc.SCHEDULE_PERSISTENT if persistent else tc.SCHEDULE_PLAIN
+    post, ok, used = decoder.decode(KS, llr, FILLERS, tc.DecodeOptions(
+        8, True, 0, -1, sched, convention=tc.CONVENTION_3GPP))
+    lo = po = 0
+    flags = []
+    for i, k in enumerate(KS):
+        ref, rok, rused = oracle.std_decode_cb(k, FILLERS[i], llr[lo:lo + 3 * (k + 4)], 8, True,
+                                               window=schedule_window(k, persistent), guard=96)
+        assert (bool(ok[i]), int(used[i])) == (rok, rused), (i, k)
+        err, hard = llr_close(post[po:po + k], ref)
+        assert err <= 1e-3 and hard == 0, (i, k, err)
+        flags.append(rok)
+        lo += 3 * (k + 4)
+        po += k
+    assert any(flags) and not all(flags), flags  # both branches of the early stop ran
+
+
+def test_std_full_trellis_matches_oracle(tc, decoder, oracle):
+    llr, _ = std_code_blocks(tc, [40, 1056, 6144], 1.0, seed=4)
+    post, ok, used = decoder.decode([40, 1056, 6144], llr, None, tc.DecodeOptions(
+        6, False, 6144, -1, convention=tc.CONVENTION_3GPP))
+    lo = po = 0
+    for k in (40, 1056, 6144):
+        ref, _, _ = oracle.std_decode_cb(k, 0, llr[lo:lo + 3 * (k + 4)], 6)
+        err, hard = llr_close(post[po:po + k], ref)
+        assert err <= 1e-3 and hard == 0, (k, err)
+        lo += 3 * (k + 4)
+        po += k
+
+
+def test_convention_selects_the_code(tc, decoder):
+    """At 3 dB every 36.212 block decodes under its own convention and (nearly) none under the
+    reference's; the same holds for the reference's blocks the other way round."""
+    ks = [1056] * 24 + [6144] * 8
+    std_llr, std_cb = std_code_blocks(tc, ks, 3.0, seed=5)
+    bits, ref_llr = tc.awgn_code_blocks(6, ks, 3.0, None, True)
+    for llr, conv, other in ((std_llr, tc.CONVENTION_3GPP, tc.CONVENTION_REFERENCE),
+                             (ref_llr, tc.CONVENTION_REFERENCE, tc.CONVENTION_3GPP)):
+        _, ok, _ = decoder.decode(ks, llr, None, tc.DecodeOptions(8, True, convention=conv))
+        assert ok.all()
+        _, ok_other, it = decoder.decode(ks, llr, None,
+                                         tc.DecodeOptions(8, True, convention=other))
+        assert ok_other.sum() <= 1 and (it[~ok_other] == 8).all()
+    post, ok, _ = decoder.decode(ks, std_llr, None, tc.DecodeOptions(
+        8, True, schedule=tc.SCHEDULE_PERSISTENT, convention=tc.CONVENTION_3GPP))
+    assert ok.all() and np.array_equal((post >= 0).astype(np.uint8), np.concatenate(std_cb))
+
+
+def test_graphs_keep_the_conventions_apart(tc, decoder):
+    import torch
+
+    ks = [512, 6144, 2048]
+    llr, _ = std_code_blocks(tc, ks, 0.5, seed=7)
+    cbs, llr_len, post_len = tc.Decoder.layout(ks)
+    x = torch.from_numpy(llr).cuda()
+    s = torch.cuda.Stream()
+    p = torch.zeros(post_len, device="cuda")
+    out = {}
+    for conv in (tc.CONVENTION_3GPP, tc.CONVENTION_REFERENCE, tc.CONVENTION_3GPP):
+        for graph in (False, True, True):
+            p.zero_()
+            torch.cuda.synchronize()
+            decoder.decode_device(cbs, len(ks), x.data_ptr(), llr_len, p.data_ptr(), post_len,
+                                  options=tc.DecodeOptions(6, False, graph=graph,
+                                                           convention=conv),
+                                  stream=s.cuda_stream)
+            s.synchronize()
+            out.setdefault(conv, []).append(p.cpu().numpy())
+    for conv, runs in out.items():
+        for r in runs[1:]:
+            assert np.array_equal(r, runs[0]), conv
+    assert not np.array_equal(out[tc.CONVENTION_3GPP][0], out[tc.CONVENTION_REFERENCE][0])
+
+
+@pytest.mark.parametrize("persistent", [False, True])
+def test_std_transport_blocks_through_the_device_chain(tc, decoder, persistent):
+    tbs, blocks, llrs, truth = [], [], [], []
+    for t, (size, rate) in enumerate([(1000, 0.5), (20000, 0.6), (6104, 0.4), (60000, 0.6)]):
+        g = int(np.ceil(size / rate / 2.0)) * 2
+        p = tc.LteTurboCodecParams(transport_block_bits=size, g_total=g,
+                                   convention=tc.CONVENTION_3GPP)
+        bits = tc.random_bits(100 + t, size)
+        enc = tc.encode_transport_block(p, bits)
+        rm = np.concatenate([b.rate_matched_bits for b in enc.code_blocks])
+        sigma2 = 1.0 / (2.0 * (size / g) * 10 ** (3.0 / 10.0))
+        llrs.append(tc.awgn_llr(200 + t, rm, sigma2))
+        blocks += [(b.descriptor.k_r, b.descriptor.filler_count, b.descriptor.e_r, 0)
+                   for b in enc.code_blocks]
+        tbs.append((size, len(enc.code_blocks)))
+        truth.append(bits)
+    e_llr = np.concatenate(llrs)
+    sched = tc.SCHEDULE_PERSISTENT if persistent else tc.SCHEDULE_PLAIN
+    got, tb_ok, cb_ok, it = decoder.decode_tbs(tbs, blocks, e_llr, tc.DecodeOptions(
+        8, True, schedule=sched, convention=tc.CONVENTION_3GPP))
+    assert tb_ok.all() and cb_ok.all() and (it >= 1).all()
+    for g_bits, t_bits in zip(got, truth):
+        assert np.array_equal(g_bits, t_bits)
+    # the same LLRs under the reference's code: no transport block passes its CRC24A
+    _, tb_bad, _, _ = decoder.decode_tbs(tbs, blocks, e_llr,
+                                         tc.DecodeOptions(8, True, schedule=sched))
+    assert not tb_bad.any()
+
+
+def test_std_reference_api_round_trip(tc):
+    """encode_transport_block / decode_transport_block with LteTurboCodecParams.convention."""
+    for size in (40, 5000, 14112):
+        g = 3 * (size + 100)
+        p = tc.LteTurboCodecParams(transport_block_bits=size, g_total=g, max_iterations=6,
+                                   convention=tc.CONVENTION_3GPP)
+        bits = tc.random_bits(size, size)
+        enc = tc.encode_transport_block(p, bits)
+        for be in (tc.DecoderBackend.GpuStage1Exact, tc.DecoderBackend.GpuB200Persistent):
+            dec = tc.decode_transport_block(p, enc, be)
+            assert dec.transport_block_crc_ok and all(dec.code_block_crc_ok)
+            assert np.array_equal(dec.tb_bits, bits)
+
+
+def test_graph_on_the_legacy_stream_is_refused(tc, decoder):
+    """The legacy default stream cannot be captured: refused before any capture starts, and the
+    decoder (and the same request on a created stream) works afterwards."""
+    import torch
+
+    ks = [1056, 40]
+    llr, _ = std_code_blocks(tc, ks, 1.0, seed=8)
+    cbs, llr_len, post_len = tc.Decoder.layout(ks)
+    x = torch.from_numpy(llr).cuda()
+    p = torch.zeros(post_len, device="cuda")
+    opts = tc.DecodeOptions(4, graph=True, convention=tc.CONVENTION_3GPP)
+    with pytest.raises(tc.InvalidArgument):
+        decoder.decode_device(cbs, len(ks), x.data_ptr(), llr_len, p.data_ptr(), post_len,
+                              options=opts)
+    ref = decoder.decode(ks, llr, None, tc.DecodeOptions(4, convention=tc.CONVENTION_3GPP))[0]
+    s = torch.cuda.Stream()
+    decoder.decode_device(cbs, len(ks), x.data_ptr(), llr_len, p.data_ptr(), post_len,
+                          options=opts, stream=s.cuda_stream)
+    s.synchronize()
+    assert np.array_equal(p.cpu().numpy(), ref)

@@ -34,6 +34,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libturbo_b200.so")
 
 MEM_HOST, MEM_DEVICE, MEM_HOST_ASYNC = 0, 1, 2
 SCHEDULE_PLAIN, SCHEDULE_PERSISTENT, SCHEDULE_AUTO = 0, 1, 2
+CONVENTION_REFERENCE, CONVENTION_3GPP = 0, 1  # the reference's code; TS 36.212 (new)
 
 
 # ------------------------------------------------------------------------------------------
@@ -79,7 +80,8 @@ class _CodeBlock(C.Structure):
 class _Options(C.Structure):
     _fields_ = [("max_iterations", C.c_uint32), ("early_stop", C.c_uint32), ("window", C.c_int32),
                 ("guard", C.c_int32), ("memory", C.c_uint32), ("schedule", C.c_uint32),
-                ("scales", C.c_void_p), ("graph", C.c_uint32), ("stream", C.c_void_p)]
+                ("scales", C.c_void_p), ("graph", C.c_uint32), ("stream", C.c_void_p),
+                ("convention", C.c_uint32)]
 
 
 class _RmBlock(C.Structure):
@@ -125,6 +127,10 @@ _SIGNATURES = {
     "tc_crc_check": [C.c_int, _VP, _SZ, _VP],
     "tc_segment_transport_block": [_VP, _SZ, _VP, _VP, _SZ],
     "tc_turbo_encode": [_I32, _I32, _VP, _VP],
+    "tc_crc_append_conv": [C.c_int, C.c_int, _VP, _SZ, _VP],
+    "tc_crc_check_conv": [C.c_int, C.c_int, _VP, _SZ, _VP],
+    "tc_segment_transport_block_conv": [C.c_int, _VP, _SZ, _VP, _VP, _SZ],
+    "tc_turbo_encode_conv": [C.c_int, _I32, _I32, _VP, _VP],
     "tc_compute_e": [_SZ, _SZ, _SZ, _U32, _U32, _VP],
     "tc_rate_match": [_I32, _I32, _VP, _SZ, _U32, _VP],
     "tc_derate_match_bits": [_I32, _I32, _VP, _SZ, _U32, _VP],
@@ -251,28 +257,29 @@ def qpp_inverse_permutation(k: int) -> np.ndarray:
 _CRC_LEN = (24, 24, 16, 8)
 
 
-def _crc_append(kind: int, bits) -> np.ndarray:
+def _crc_append(kind: int, bits, convention: int = CONVENTION_REFERENCE) -> np.ndarray:
     b = _u8(bits)
     out = np.empty(b.size + _CRC_LEN[kind], np.uint8)
-    _call("tc_crc_append", kind, _ptr(b), b.size, _ptr(out))
+    _call("tc_crc_append_conv", int(convention), kind, _ptr(b), b.size, _ptr(out))
     return out
 
 
-def _crc_check(kind: int, bits) -> bool:
+def _crc_check(kind: int, bits, convention: int = CONVENTION_REFERENCE) -> bool:
     b = _u8(bits)
     ok = C.c_int()
-    _call("tc_crc_check", kind, _ptr(b), b.size, C.addressof(ok))
+    _call("tc_crc_check_conv", int(convention), kind, _ptr(b), b.size, C.addressof(ok))
     return bool(ok.value)
 
 
-def append_crc24a(bits): return _crc_append(0, bits)
-def append_crc24b(bits): return _crc_append(1, bits)
-def append_crc16(bits): return _crc_append(2, bits)
-def append_crc8(bits): return _crc_append(3, bits)
-def check_crc24a(bits): return _crc_check(0, bits)
-def check_crc24b(bits): return _crc_check(1, bits)
-def check_crc16(bits): return _crc_check(2, bits)
-def check_crc8(bits): return _crc_check(3, bits)
+# convention: CONVENTION_REFERENCE (the reference's generator arrays) or CONVENTION_3GPP
+def append_crc24a(bits, convention=CONVENTION_REFERENCE): return _crc_append(0, bits, convention)
+def append_crc24b(bits, convention=CONVENTION_REFERENCE): return _crc_append(1, bits, convention)
+def append_crc16(bits, convention=CONVENTION_REFERENCE): return _crc_append(2, bits, convention)
+def append_crc8(bits, convention=CONVENTION_REFERENCE): return _crc_append(3, bits, convention)
+def check_crc24a(bits, convention=CONVENTION_REFERENCE): return _crc_check(0, bits, convention)
+def check_crc24b(bits, convention=CONVENTION_REFERENCE): return _crc_check(1, bits, convention)
+def check_crc16(bits, convention=CONVENTION_REFERENCE): return _crc_check(2, bits, convention)
+def check_crc8(bits, convention=CONVENTION_REFERENCE): return _crc_check(3, bits, convention)
 
 
 # ------------------------------------------------------------------------------------------
@@ -290,13 +297,16 @@ class SegmentationResult:
     code_blocks: list
 
 
-def segment_transport_block(bits_with_crc) -> SegmentationResult:
+def segment_transport_block(bits_with_crc, convention: int = CONVENTION_REFERENCE
+                            ) -> SegmentationResult:
     b = _u8(bits_with_crc)
     s = _Seg()
-    _call("tc_segment_transport_block", _ptr(b), b.size, C.addressof(s), None, 0)
+    conv = int(convention)
+    _call("tc_segment_transport_block_conv", conv, _ptr(b), b.size, C.addressof(s), None, 0)
     total = s.c_plus * s.k_plus + s.c_minus * s.k_minus
     cbs = np.empty(total, np.uint8)
-    _call("tc_segment_transport_block", _ptr(b), b.size, C.addressof(s), _ptr(cbs), cbs.size)
+    _call("tc_segment_transport_block_conv", conv, _ptr(b), b.size, C.addressof(s), _ptr(cbs),
+          cbs.size)
     blocks, pos = [], 0
     for r in range(s.c):
         kr = s.k_minus if r < s.c_minus else s.k_plus
@@ -340,6 +350,7 @@ class LteTurboCodecParams:
     n_soft: int = 0
     max_iterations: int = 8
     enable_early_stop: bool = False
+    convention: int = 0  # CONVENTION_REFERENCE; CONVENTION_3GPP: the TS 36.212 code (new)
 
 
 @dataclass
@@ -379,13 +390,15 @@ class DecodedTransportBlock:
     posterior_llr: Optional[np.ndarray]
 
 
-def turbo_encode_code_block(descriptor: CodeBlockDescriptor, cb_bits) -> EncodedCodeBlock:
+def turbo_encode_code_block(descriptor: CodeBlockDescriptor, cb_bits,
+                            convention: int = CONVENTION_REFERENCE) -> EncodedCodeBlock:
     b = _u8(cb_bits)
     k = int(descriptor.k_r)
     if b.size != k:
         raise InvalidArgument("code block length mismatch")
     d = np.empty(3 * (k + 4), np.uint8)
-    _call("tc_turbo_encode", k, int(descriptor.filler_count), _ptr(b), _ptr(d))
+    _call("tc_turbo_encode_conv", int(convention), k, int(descriptor.filler_count), _ptr(b),
+          _ptr(d))
     desc = CodeBlockDescriptor(descriptor.block_index, k, k + 4, descriptor.e_r,
                                descriptor.filler_count, qpp_index(k))
     return EncodedCodeBlock(desc, b.copy(), d[:k + 4].copy(), d[k + 4:2 * k + 8].copy(),
@@ -410,8 +423,9 @@ def encode_transport_block(params: LteTurboCodecParams, transport_bits) -> Encod
     bits = _u8(transport_bits)
     if params.transport_block_bits != bits.size:
         raise InvalidArgument("transport block size does not match params")
-    with_crc = append_crc24a(bits)
-    seg = segment_transport_block(with_crc)
+    conv = int(params.convention)
+    with_crc = append_crc24a(bits, conv)
+    seg = segment_transport_block(with_crc, conv)
     blocks = []
     for r, cb in enumerate(seg.code_blocks):
         k = cb.size
@@ -419,7 +433,7 @@ def encode_transport_block(params: LteTurboCodecParams, transport_bits) -> Encod
                                    compute_e(r, params.g_total, seg.c, params.num_layers,
                                              params.mod_order),
                                    seg.filler_bits if r == 0 else 0, qpp_index(k))
-        enc = turbo_encode_code_block(desc, cb)
+        enc = turbo_encode_code_block(desc, cb, conv)
         d012 = np.concatenate([enc.systematic, enc.parity0, enc.parity1])
         enc.rate_matched_bits = rate_match(k, desc.filler_count, d012, desc.e_r, params.rv)
         blocks.append(enc)
@@ -485,6 +499,7 @@ class DecodeOptions:
     schedule: int = SCHEDULE_PLAIN
     scales: Optional[Sequence[float]] = None  # 2 per iteration; None = 1.0
     graph: bool = False      # device memory: capture once, replay the CUDA graph
+    convention: int = 0      # CONVENTION_REFERENCE; CONVENTION_3GPP: LLRs of the TS 36.212 code
 
 
 class Decoder:
@@ -526,6 +541,7 @@ class Decoder:
             opt.scales = keep.ctypes.data
         opt.graph = int(bool(o.graph))
         opt.stream = stream or None
+        opt.convention = int(o.convention)
         return opt, keep
 
     def inject_stall(self, task: int) -> None:
@@ -813,8 +829,10 @@ def decode_transport_block(params: LteTurboCodecParams, encoded: EncodedTranspor
                           for b in blocks])
     window = 6144 if backend == DecoderBackend.GpuStage1Exact else 0
     schedule = SCHEDULE_PERSISTENT if backend == DecoderBackend.GpuB200Persistent else SCHEDULE_PLAIN
+    conv = int(params.convention)
     post, ok, it = _decoder().decode(ks, llr, fillers, DecodeOptions(
-        params.max_iterations, params.enable_early_stop, window, -1, schedule))
+        params.max_iterations, params.enable_early_stop, window, -1, schedule,
+        convention=conv))
     tb, cb_ok, pos = [], [], 0
     for b in blocks:
         k = b.descriptor.k_r
@@ -822,10 +840,10 @@ def decode_transport_block(params: LteTurboCodecParams, encoded: EncodedTranspor
         pos += k
         good = True
         if len(blocks) > 1:
-            good = check_crc24b(hard)
+            good = check_crc24b(hard, conv)
             hard = hard[:-24]
         tb.append(hard)
         cb_ok.append(good)
     tb_bits = np.concatenate(tb) if tb else np.zeros(0, np.uint8)
-    return DecodedTransportBlock(tb_bits[:-24].copy(), cb_ok, check_crc24a(tb_bits),
+    return DecodedTransportBlock(tb_bits[:-24].copy(), cb_ok, check_crc24a(tb_bits, conv),
                                  int(it.max()) if len(it) else 0, post)

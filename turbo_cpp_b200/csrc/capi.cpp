@@ -57,6 +57,11 @@ tcb::CrcKind crc_kind(int kind) {
   return static_cast<tcb::CrcKind>(kind);
 }
 
+tcb::Convention convention_of(int c) {
+  need(c == TC_CONVENTION_REFERENCE || c == TC_CONVENTION_3GPP, "unknown convention");
+  return c == TC_CONVENTION_3GPP ? tcb::Convention::Std3gpp : tcb::Convention::Reference;
+}
+
 }  // namespace
 
 struct tc_decoder {
@@ -126,25 +131,34 @@ int tc_qpp_inverse_permutation(int32_t k, int32_t* inv) {
   });
 }
 
-int tc_crc_append(int kind, const uint8_t* bits, size_t n, uint8_t* out) {
+int tc_crc_append_conv(int convention, int kind, const uint8_t* bits, size_t n, uint8_t* out) {
   return guarded([&] {
     need(out != nullptr && (bits != nullptr || n == 0), "null pointer");
-    tcb::crc_append(crc_kind(kind), bits, n, out);
+    tcb::crc_append(crc_kind(kind), bits, n, out, convention_of(convention));
+  });
+}
+
+int tc_crc_append(int kind, const uint8_t* bits, size_t n, uint8_t* out) {
+  return tc_crc_append_conv(TC_CONVENTION_REFERENCE, kind, bits, n, out);
+}
+
+int tc_crc_check_conv(int convention, int kind, const uint8_t* bits, size_t n, int* ok) {
+  return guarded([&] {
+    need(ok != nullptr && (bits != nullptr || n == 0), "null pointer");
+    *ok = tcb::crc_check(crc_kind(kind), bits, n, convention_of(convention)) ? 1 : 0;
   });
 }
 
 int tc_crc_check(int kind, const uint8_t* bits, size_t n, int* ok) {
-  return guarded([&] {
-    need(ok != nullptr && (bits != nullptr || n == 0), "null pointer");
-    *ok = tcb::crc_check(crc_kind(kind), bits, n) ? 1 : 0;
-  });
+  return tc_crc_check_conv(TC_CONVENTION_REFERENCE, kind, bits, n, ok);
 }
 
-int tc_segment_transport_block(const uint8_t* bits, size_t b, tc_segmentation* info,
-                               uint8_t* cb_bits, size_t cap) {
+int tc_segment_transport_block_conv(int convention, const uint8_t* bits, size_t b,
+                                    tc_segmentation* info, uint8_t* cb_bits, size_t cap) {
   return guarded([&] {
     need(info != nullptr, "null output pointer");
     need(bits != nullptr || b == 0, "null input");
+    const tcb::Convention conv = convention_of(convention);
     const tcb::Segmentation s = tcb::segment_sizes(b);
     info->c = s.c;
     info->c_plus = s.c_plus;
@@ -155,18 +169,29 @@ int tc_segment_transport_block(const uint8_t* bits, size_t b, tc_segmentation* i
     info->l = s.l;
     if (cb_bits) {
       need(cap >= s.total_bits(), "code-block buffer too small");
-      tcb::segment_bits(bits, b, s, cb_bits);
+      tcb::segment_bits(bits, b, s, cb_bits, conv);
     }
   });
 }
 
-int tc_turbo_encode(int32_t k, int32_t filler, const uint8_t* cb_bits, uint8_t* d012) {
+int tc_segment_transport_block(const uint8_t* bits, size_t b, tc_segmentation* info,
+                               uint8_t* cb_bits, size_t cap) {
+  return tc_segment_transport_block_conv(TC_CONVENTION_REFERENCE, bits, b, info, cb_bits, cap);
+}
+
+int tc_turbo_encode_conv(int convention, int32_t k, int32_t filler, const uint8_t* cb_bits,
+                         uint8_t* d012) {
   return guarded([&] {
     need(cb_bits && d012, "null pointer");
+    const tcb::Convention conv = convention_of(convention);
     if (tcb::qpp_index(k) < 0) throw tcb::OutOfRange("unsupported QPP block size");
     need(filler >= 0 && filler < k, "invalid filler count");
-    tcb::turbo_encode(k, filler, cb_bits, d012);
+    tcb::turbo_encode(k, filler, cb_bits, d012, conv);
   });
+}
+
+int tc_turbo_encode(int32_t k, int32_t filler, const uint8_t* cb_bits, uint8_t* d012) {
+  return tc_turbo_encode_conv(TC_CONVENTION_REFERENCE, k, filler, cb_bits, d012);
 }
 
 int tc_compute_e(size_t r, size_t g_total, size_t c, uint32_t num_layers, uint32_t mod_order,
@@ -291,6 +316,7 @@ int tc_decode(tc_decoder* dec, size_t n_cb, const tc_code_block* cbs, size_t llr
     rq.graph = o.graph != 0;
     rq.scales = o.scales;
     rq.stream = o.stream;
+    rq.std3gpp = convention_of(static_cast<int>(o.convention)) == tcb::Convention::Std3gpp;
     dec->impl.decode(rq);
   });
 }
@@ -304,6 +330,8 @@ int tc_decode_noalloc(size_t n_cb, const tc_code_block* cbs, size_t llr_len, con
     tc_decode_options o;
     if (opts) o = *opts; else tc_decode_options_init(&o);
     need(o.max_iterations <= 64, "max_iterations above 64");
+    need(o.convention == TC_CONVENTION_REFERENCE,
+         "tc_decode_noalloc decodes the reference convention only");
     tcb::DecodeRequest rq;
     rq.n_cb = n_cb;
     rq.cbs = reinterpret_cast<const tcb::CodeBlockDesc*>(cbs);
@@ -345,6 +373,7 @@ int tc_autotune(tc_decoder* dec, size_t n_cb, const tc_code_block* cbs, size_t l
     rq.device_memory = true;
     rq.scales = o.scales;
     rq.stream = o.stream;
+    rq.std3gpp = convention_of(static_cast<int>(o.convention)) == tcb::Convention::Std3gpp;
     const auto c = dec->impl.autotune(rq);
     if (best) {
       best->schedule = c.persistent ? TC_SCHEDULE_PERSISTENT : TC_SCHEDULE_PLAIN;
@@ -468,6 +497,7 @@ int tc_decode_transport_blocks(tc_decoder* dec, size_t n_tb, const tc_transport_
     q.decode.guard = o.guard;
     q.decode.persistent = o.schedule == TC_SCHEDULE_PERSISTENT;
     q.decode.scales = o.scales;
+    q.decode.std3gpp = convention_of(static_cast<int>(o.convention)) == tcb::Convention::Std3gpp;
     dec->impl.decode_transport_blocks(q);
   });
 }

@@ -147,9 +147,9 @@ __global__ void tb_finish_kernel(const DevTb* __restrict__ tbs, int n_tb, const 
   if (lane == 0) tb_ok[warp] = (pos == n_a) && syn_a == 0;
 }
 
-std::vector<uint32_t> xpow_table(CrcKind kind, size_t n) {
+std::vector<uint32_t> xpow_table(CrcKind kind, size_t n, Convention conv) {
   std::vector<uint32_t> t(n);
-  const uint32_t g = crc_generator_mask(kind);
+  const uint32_t g = crc_generator_mask(kind, conv);
   uint32_t r = 1;
   for (size_t j = 0; j < n; ++j) {
     t[j] = r;
@@ -288,14 +288,16 @@ void Decoder::decode_transport_blocks(const TbRequest& q) {
   uint32_t* iters = q.device_memory && q.iterations_used ? q.iterations_used
                                                          : grow<uint32_t>(d_tbiters_, q.n_cb);
   DevTb* dtb = grow<DevTb>(d_tb_, q.n_tb);
-  if (d_xpow_a_.bytes == 0) {
-    const auto xa = xpow_table(CrcKind::Crc24A, 6144 * 17);  // > largest TB + CRC24A
-    const auto xb = xpow_table(CrcKind::Crc24B, 6144);
-    d_xpow_a_.reserve(xa.size() * 4);
-    check(cudaMemcpy(d_xpow_a_.ptr, xa.data(), xa.size() * 4, cudaMemcpyHostToDevice), "upload crc");
+  const bool std3gpp = q.decode.std3gpp;
+  DeviceBuffer& xpow_a = std3gpp ? d_xpow_a_std_ : d_xpow_a_;  // x^j mod g_CRC24A
+  if (xpow_a.bytes == 0) {
+    const auto xa = xpow_table(CrcKind::Crc24A, 6144 * 17,  // > largest TB + CRC24A
+                               std3gpp ? Convention::Std3gpp : Convention::Reference);
+    xpow_a.reserve(xa.size() * 4);
+    check(cudaMemcpy(xpow_a.ptr, xa.data(), xa.size() * 4, cudaMemcpyHostToDevice), "upload crc");
   }
   for (size_t t = 0; t < q.n_tb; ++t)
-    if (tbs[t].tbs + 24 > static_cast<int64_t>(d_xpow_a_.bytes / 4))
+    if (tbs[t].tbs + 24 > static_cast<int64_t>(xpow_a.bytes / 4))
       throw CapacityExceeded("transport block larger than 104424 bits");
   // ---- de-rate matching, decoding, transport-block finish ----
   derate_device(q.n_cb, rm.data(), e_llr, q.e_len, d012, static_cast<size_t>(llr_len), st);
@@ -316,7 +318,8 @@ void Decoder::decode_transport_blocks(const TbRequest& q) {
   upload(dtb, tbs.data(), q.n_tb * sizeof(DevTb), st);
   tb_finish_kernel<<<static_cast<unsigned>((q.n_tb * 32 + 255) / 256), 256, 0, st>>>(
       dtb, static_cast<int>(q.n_tb), static_cast<const DevCb*>(d_cbs_.ptr), post,
-      static_cast<const uint32_t*>(d_xpow_a_.ptr), static_cast<const uint32_t*>(d_xpow_.ptr), bits,
+      static_cast<const uint32_t*>(xpow_a.ptr),
+      static_cast<const uint32_t*>(std3gpp ? d_xpow_std_.ptr : d_xpow_.ptr), bits,
       tb_ok, cb_ok);
   check(cudaGetLastError(), "finish launch");
   timing_.launches += 1;

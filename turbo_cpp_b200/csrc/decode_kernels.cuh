@@ -16,8 +16,9 @@ namespace {
 constexpr int kThreads = 64;  // threads (windows) per block of the plain SISO kernel
 constexpr int kMinBlocks = 10;  // 20 warps per SM: at most 96 registers per thread
 
-// KIND: 0 = upper SISO, 1 = lower SISO, 2 = lower SISO that also writes the posterior
-template <int S, int KIND, bool GLOBAL_CKPT>
+// KIND: 0 = upper SISO, 1 = lower SISO, 2 = lower SISO that also writes the posterior;
+// STD: the TS 36.212 code instead of the reference's
+template <int S, int KIND, bool GLOBAL_CKPT, bool STD = false>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) siso_plain_kernel(const DevCb* __restrict__ cbs,
                                                               const int32_t* __restrict__ win_cb,
                                                               int n_win, SisoIo io,
@@ -33,10 +34,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) siso_plain_kernel(const 
   const int w = g - cb.win0;
   if (GLOBAL_CKPT) {
     CkptGlobal ck{ckpt_global + static_cast<int64_t>(2) * ckpt_per_thread * g};
-    siso_window<S, KIND != 0, KIND == 2>(cb, w, g, io, ck);
+    siso_window<S, KIND != 0, KIND == 2, CkptGlobal, false, STD>(cb, w, g, io, ck);
   } else {
     CkptSmem ck{smem_ckpt, static_cast<int>(blockDim.x), static_cast<int>(threadIdx.x)};
-    siso_window<S, KIND != 0, KIND == 2>(cb, w, g, io, ck);
+    siso_window<S, KIND != 0, KIND == 2, CkptSmem, false, STD>(cb, w, g, io, ck);
   }
 }
 
@@ -155,6 +156,7 @@ __device__ __forceinline__ void store_release(int* p, int v) {
   asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+template <bool STD = false>
 __global__ void __launch_bounds__(kPersistThreads, kPersistMinBlocks)
     persistent_kernel(const PersistArgs p) {
   const int lane = threadIdx.x & 31;
@@ -195,7 +197,8 @@ __global__ void __launch_bounds__(kPersistThreads, kPersistMinBlocks)
                     : SisoIo{p.llr, p.sys_i, p.e1i, p.e2, p.post, p.perm, p.inv, p.seed_lo[it & 1],
                              p.seed_lo[(it + 1) & 1], p.scale[2 * it + 1], p.guard};
       if (active)
-        siso_window_rt<kSub, CkptGlobal, true>(cb, w, g, io, ck, half == 1, half == 1 && post_now);
+        siso_window_rt<kSub, CkptGlobal, true, STD>(cb, w, g, io, ck, half == 1,
+                                                    half == 1 && post_now);
       if (half == 1 && p.early_stop) {
         // CRC24B syndrome of the hard decisions (lte_turbo.cpp:792-804): each lane XORs
         // x^(N-1-i) mod g over the set bits of its window; a block's windows sit in consecutive

@@ -121,26 +121,47 @@ Decoder::Decoder(int device) : device_(device) {
   check(cudaMemcpy(d_perm_.ptr, perm.data(), perm.size() * 2, cudaMemcpyHostToDevice), "upload perm");
   check(cudaMemcpy(d_inv_.ptr, inv.data(), inv.size() * 2, cudaMemcpyHostToDevice), "upload inv");
   check(cudaMemcpy(d_xpow_.ptr, xpow.data(), xpow.size() * 4, cudaMemcpyHostToDevice), "upload crc");
+  {  // the same for TS 36.212's CRC24B
+    const uint32_t gs = crc_generator_mask(CrcKind::Crc24B, Convention::Std3gpp);
+    uint32_t q = 1;
+    for (int j = 0; j < 6144; ++j) {
+      xpow[j] = q;
+      q <<= 1;
+      if (q & (1u << 24)) q ^= (1u << 24) | gs;
+    }
+    d_xpow_std_.reserve(xpow.size() * 4);
+    check(cudaMemcpy(d_xpow_std_.ptr, xpow.data(), xpow.size() * 4, cudaMemcpyHostToDevice),
+          "upload crc");
+  }
   d_err_.reserve(sizeof(int));
   check(cudaMemset(d_err_.ptr, 0, sizeof(int)), "zero error word");
 
   const int smem = smem_optin_;
-  check(cudaFuncSetAttribute(siso_plain_kernel<kSub, 0, false>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
-  check(cudaFuncSetAttribute(siso_plain_kernel<kSub, 1, false>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
-  check(cudaFuncSetAttribute(siso_plain_kernel<kSub, 2, false>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
+  for (const void* f : {reinterpret_cast<const void*>(siso_plain_kernel<kSub, 0, false>),
+                        reinterpret_cast<const void*>(siso_plain_kernel<kSub, 1, false>),
+                        reinterpret_cast<const void*>(siso_plain_kernel<kSub, 2, false>),
+                        reinterpret_cast<const void*>(siso_plain_kernel<kSub, 0, false, true>),
+                        reinterpret_cast<const void*>(siso_plain_kernel<kSub, 1, false, true>),
+                        reinterpret_cast<const void*>(siso_plain_kernel<kSub, 2, false, true>)})
+    check(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
   for (const void* f : {reinterpret_cast<const void*>(siso_plain_kernel<kSub, 0, true>),
                         reinterpret_cast<const void*>(siso_plain_kernel<kSub, 1, true>),
-                        reinterpret_cast<const void*>(siso_plain_kernel<kSub, 2, true>)})
+                        reinterpret_cast<const void*>(siso_plain_kernel<kSub, 2, true>),
+                        reinterpret_cast<const void*>(siso_plain_kernel<kSub, 0, true, true>),
+                        reinterpret_cast<const void*>(siso_plain_kernel<kSub, 1, true, true>),
+                        reinterpret_cast<const void*>(siso_plain_kernel<kSub, 2, true, true>),
+                        reinterpret_cast<const void*>(persistent_kernel<false>),
+                        reinterpret_cast<const void*>(persistent_kernel<true>)})
     check(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 0),
           "carveout attr");
-  check(cudaFuncSetAttribute(persistent_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 0),
-        "carveout attr");
-  check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&persist_blocks_per_sm_, persistent_kernel,
+  int per_sm_std = 0;
+  check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_std, persistent_kernel<true>,
                                                       kPersistThreads, 0),
         "occupancy");
+  check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&persist_blocks_per_sm_, persistent_kernel<false>,
+                                                      kPersistThreads, 0),
+        "occupancy");
+  persist_blocks_per_sm_ = std::min(persist_blocks_per_sm_, per_sm_std);
 }
 
 Decoder::~Decoder() {
@@ -154,7 +175,7 @@ Decoder::~Decoder() {
   }
   workers_.clear();  // each waits for its own work (cudaFree) and releases its buffers
   if (stream_) cudaStreamDestroy(static_cast<cudaStream_t>(stream_));
-  for (DeviceBuffer* b : {&d_perm_, &d_inv_, &d_xpow_, &d_cbs_, &d_wincb_, &d_start_, &d_llr_,
+  for (DeviceBuffer* b : {&d_perm_, &d_inv_, &d_xpow_, &d_xpow_std_, &d_xpow_a_std_, &d_cbs_, &d_wincb_, &d_start_, &d_llr_,
                           &d_sysi_, &d_e1i_, &d_e2_, &d_post_, &d_seed_, &d_done_, &d_iters_,
                           &d_crc_, &d_ckpt_, &d_tasks_, &d_queue_, &d_rm_, &d_e_llr_, &d_d012_,
                           &d_tbpost_, &d_tbbits_, &d_tbok_, &d_cbok_, &d_tbiters_, &d_tb_,
@@ -282,7 +303,7 @@ std::string Decoder::signature(const DecodeRequest& rq) {
   const int n_log2 = rq.n_cb ? static_cast<int>(std::lround(std::log2(static_cast<double>(rq.n_cb)))) : 0;
   std::ostringstream o;
   o << "es=" << (rq.early_stop ? 1 : 0) << ",it=" << rq.max_iterations << ",n~2^" << n_log2
-    << ",meanK~" << mean_k << ",guard=" << rq.guard;
+    << ",meanK~" << mean_k << ",guard=" << rq.guard << (rq.std3gpp ? ",std3gpp" : "");
   return o.str();
 }
 
@@ -407,6 +428,8 @@ void Decoder::decode_graph(const DecodeRequest& rq) {
   std::lock_guard<std::mutex> lock(mu_);
   check(cudaSetDevice(device_), "cudaSetDevice");
   cudaStream_t st = static_cast<cudaStream_t>(rq.stream);
+  if (st == nullptr || st == cudaStreamLegacy)
+    throw InvalidArgument("graph: the legacy default stream cannot be captured; pass a created stream");
   std::string key;
   auto put = [&key](const void* p, size_t n) { key.append(static_cast<const char*>(p), n); };
   const uintptr_t ptrs[4] = {reinterpret_cast<uintptr_t>(rq.llr),
@@ -415,7 +438,8 @@ void Decoder::decode_graph(const DecodeRequest& rq) {
                              reinterpret_cast<uintptr_t>(rq.iterations_used)};
   const int64_t opts[8] = {static_cast<int64_t>(rq.n_cb), static_cast<int64_t>(rq.llr_len),
                            static_cast<int64_t>(rq.post_len), rq.max_iterations, rq.early_stop,
-                           rq.window, rq.guard, (rq.persistent ? 2 : 0) | (rq.smem_checkpoints ? 1 : 0)};
+                           rq.window, rq.guard,
+                           (rq.std3gpp ? 4 : 0) | (rq.persistent ? 2 : 0) | (rq.smem_checkpoints ? 1 : 0)};
   put(ptrs, sizeof ptrs);
   put(opts, sizeof opts);
   put(rq.cbs, rq.n_cb * sizeof(CodeBlockDesc));
@@ -451,25 +475,31 @@ void Decoder::decode_graph(const DecodeRequest& rq) {
     timing_on_ = false;
     capturing_ = &e;
     cudaGraph_t g = nullptr;
-    check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    // any failure from here on removes the half-made entry, so that no later call replays it
+    cudaGraphExec_t exec = nullptr;
     try {
-      if (rq.persistent) decode_persistent(rq); else decode_plain(rq);
+      check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+      try {
+        if (rq.persistent) decode_persistent(rq); else decode_plain(rq);
+      } catch (...) {
+        cudaStreamEndCapture(st, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      check(cudaStreamEndCapture(st, &g), "cudaStreamEndCapture");
+      const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+      cudaGraphDestroy(g);
+      check(ie, "cudaGraphInstantiate");
     } catch (...) {
-      cudaStreamEndCapture(st, &g);
-      if (g) cudaGraphDestroy(g);
       capturing_ = nullptr;
       timing_on_ = timing_was;
+      timing_.launches = launches_before;
       drop_graph(e);
       graphs_.pop_front();
       throw;
     }
-    check(cudaStreamEndCapture(st, &g), "cudaStreamEndCapture");
     capturing_ = nullptr;
     timing_on_ = timing_was;
-    cudaGraphExec_t exec = nullptr;
-    const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
-    cudaGraphDestroy(g);
-    check(ie, "cudaGraphInstantiate");
     e.exec = exec;
     e.generation = generation_;
     e.launches = timing_.launches - launches_before;
@@ -485,6 +515,24 @@ void Decoder::decode_graph(const DecodeRequest& rq) {
   mark_done(st);
   timing_.launches += hit->launches;
 }
+
+namespace {
+// one plain-schedule SISO launch: kind 0 upper, 1 lower, 2 lower + posterior
+template <bool STD>
+void launch_plain(int kind, bool global_ckpt, int blocks, size_t smem, cudaStream_t st,
+                  const DevCb* dcbs, const int32_t* dwin, int n_win, const SisoIo& io,
+                  const uint8_t* dn, float4* ckpt, int max_ckpt) {
+  if (global_ckpt) {
+    if (kind == 0) siso_plain_kernel<kSub, 0, true, STD><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, dn, ckpt, max_ckpt);
+    else if (kind == 1) siso_plain_kernel<kSub, 1, true, STD><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, dn, ckpt, max_ckpt);
+    else siso_plain_kernel<kSub, 2, true, STD><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, dn, ckpt, max_ckpt);
+  } else {
+    if (kind == 0) siso_plain_kernel<kSub, 0, false, STD><<<blocks, kThreads, smem, st>>>(dcbs, dwin, n_win, io, dn, nullptr, 0);
+    else if (kind == 1) siso_plain_kernel<kSub, 1, false, STD><<<blocks, kThreads, smem, st>>>(dcbs, dwin, n_win, io, dn, nullptr, 0);
+    else siso_plain_kernel<kSub, 2, false, STD><<<blocks, kThreads, smem, st>>>(dcbs, dwin, n_win, io, dn, nullptr, 0);
+  }
+}
+}  // namespace
 
 void Decoder::decode_plain(const DecodeRequest& rq) {
   check(cudaSetDevice(device_), "cudaSetDevice");
@@ -601,22 +649,18 @@ void Decoder::decode_plain(const DecodeRequest& rq) {
       const SisoIo& io = half ? lo : up;
       const int kind = half == 0 ? 0 : (post_now ? 2 : 1);
       record_start(st);
-      if (global_ckpt) {
-        if (kind == 0) siso_plain_kernel<kSub, 0, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, dn, ckpt, max_ckpt);
-        else if (kind == 1) siso_plain_kernel<kSub, 1, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, dn, ckpt, max_ckpt);
-        else siso_plain_kernel<kSub, 2, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, dn, ckpt, max_ckpt);
-      } else {
-        if (kind == 0) siso_plain_kernel<kSub, 0, false><<<blocks, kThreads, smem, st>>>(dcbs, dwin, n_win, io, dn, nullptr, 0);
-        else if (kind == 1) siso_plain_kernel<kSub, 1, false><<<blocks, kThreads, smem, st>>>(dcbs, dwin, n_win, io, dn, nullptr, 0);
-        else siso_plain_kernel<kSub, 2, false><<<blocks, kThreads, smem, st>>>(dcbs, dwin, n_win, io, dn, nullptr, 0);
-      }
+      if (rq.std3gpp)
+        launch_plain<true>(kind, global_ckpt, blocks, smem, st, dcbs, dwin, n_win, io, dn, ckpt, max_ckpt);
+      else
+        launch_plain<false>(kind, global_ckpt, blocks, smem, st, dcbs, dwin, n_win, io, dn, ckpt, max_ckpt);
       check(cudaGetLastError(), "SISO launch");
       record_stop(st, static_cast<uint64_t>(work));
       timing_.launches += 1;
     }
     if (rq.early_stop) {
       crc_stop_kernel<<<static_cast<unsigned>((n * 32 + 255) / 256), 256, 0, st>>>(
-          dcbs, static_cast<int>(n), post, static_cast<const uint32_t*>(d_xpow_.ptr), done, iters,
+          dcbs, static_cast<int>(n), post,
+          static_cast<const uint32_t*>(rq.std3gpp ? d_xpow_std_.ptr : d_xpow_.ptr), done, iters,
           static_cast<int>(it));
       check(cudaGetLastError(), "CRC launch");
       timing_.launches += 1;
@@ -829,12 +873,15 @@ void Decoder::decode_persistent(const DecodeRequest& rq) {
   a.early_stop = rq.early_stop ? 1 : 0;
   a.done = done;
   a.iters = iters;
-  a.xpow = static_cast<const uint32_t*>(d_xpow_.ptr);
+  a.xpow = static_cast<const uint32_t*>(rq.std3gpp ? d_xpow_std_.ptr : d_xpow_.ptr);
   for (int i = 0; i < 2 * kMaxIterations; ++i)
     a.scale[i] = (rq.scales && i < 2 * static_cast<int>(rq.max_iterations)) ? rq.scales[i] : 1.0f;
   const int grid = std::max(1, sm_count_ * std::max(persist_blocks_per_sm_, 1));
   record_start(st);
-  persistent_kernel<<<grid, kPersistThreads, 0, st>>>(a);
+  if (rq.std3gpp)
+    persistent_kernel<true><<<grid, kPersistThreads, 0, st>>>(a);
+  else
+    persistent_kernel<false><<<grid, kPersistThreads, 0, st>>>(a);
   check(cudaGetLastError(), "persistent launch");
   record_stop(st, static_cast<uint64_t>(work) * 2 * rq.max_iterations);
   finish_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(static_cast<int>(n), done,

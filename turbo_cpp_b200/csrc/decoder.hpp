@@ -65,6 +65,7 @@ struct DecodeRequest {
   bool graph = false;       // device memory: capture the launch sequence once, replay it after
   bool auto_schedule = false;  // take schedule and window from the autotuning table
   const float* scales = nullptr;  // host; 2 per iteration (upper, lower); null = all 1
+  bool std3gpp = false;  // the TS 36.212 code (trellis, tail mapping, CRC24B) instead of the reference's
   void* stream = nullptr;
 };
 
@@ -230,10 +231,10 @@ class Decoder {
   int smem_optin_ = 0;
   void* stream_ = nullptr;  // cudaStream_t
   std::vector<int32_t> tab_offset_;
-  DeviceBuffer d_perm_, d_inv_, d_xpow_;
+  DeviceBuffer d_perm_, d_inv_, d_xpow_, d_xpow_std_;  // x^j mod g_CRC24B: reference, TS 36.212
   DeviceBuffer d_cbs_, d_wincb_, d_start_, d_llr_, d_sysi_, d_e1i_, d_e2_, d_post_, d_seed_,
       d_done_, d_iters_, d_crc_, d_ckpt_, d_tasks_, d_queue_;
-  DeviceBuffer d_rmgroup_, d_gen_, d_gentab_, d_genenc_, d_genrm_;
+  DeviceBuffer d_rmgroup_, d_gen_, d_gentab_, d_genenc_, d_genrm_, d_xpow_a_std_;
   DeviceBuffer d_rm_, d_e_llr_, d_d012_, d_tbpost_, d_tbbits_, d_tbok_, d_cbok_, d_tbiters_, d_tb_,
       d_xpow_a_;
   int persist_blocks_per_sm_ = 0;

@@ -109,17 +109,21 @@ const CrcSpec& spec(CrcKind k) {
 
 int crc_length(CrcKind kind) { return spec(kind).len; }
 
-uint32_t crc_generator_mask(CrcKind kind) {
+// TS 36.212 5.1.1: gCRC24A, gCRC24B, gCRC16, gCRC8 without the leading D^L (bit j = D^j)
+constexpr uint32_t kStdCrcMask[4] = {0x864CFBu, 0x800063u, 0x1021u, 0x9Bu};
+
+uint32_t crc_generator_mask(CrcKind kind, Convention conv) {
   const CrcSpec& s = spec(kind);
+  if (conv == Convention::Std3gpp) return kStdCrcMask[static_cast<int>(kind)];
   uint32_t m = 0;
   for (int j = 0; j < s.len; ++j)
     if (s.g[j]) m |= 1u << (s.len - 1 - j);
   return m;
 }
 
-uint32_t crc_remainder(CrcKind kind, const uint8_t* bits, size_t n) {
+uint32_t crc_remainder(CrcKind kind, const uint8_t* bits, size_t n, Convention conv) {
   const int L = spec(kind).len;
-  const uint32_t g = crc_generator_mask(kind), top = 1u << (L - 1),
+  const uint32_t g = crc_generator_mask(kind, conv), top = 1u << (L - 1),
                  mask = (L == 32) ? 0xffffffffu : ((1u << L) - 1u);
   uint32_t r = 0;
   for (size_t i = 0; i < n; ++i) {
@@ -130,17 +134,17 @@ uint32_t crc_remainder(CrcKind kind, const uint8_t* bits, size_t n) {
   return r;
 }
 
-void crc_append(CrcKind kind, const uint8_t* bits, size_t n, uint8_t* out) {
+void crc_append(CrcKind kind, const uint8_t* bits, size_t n, uint8_t* out, Convention conv) {
   const int L = crc_length(kind);
-  const uint32_t r = crc_remainder(kind, bits, n);
+  const uint32_t r = crc_remainder(kind, bits, n, conv);
   if (out != bits) std::copy(bits, bits + n, out);
   for (int j = 0; j < L; ++j) out[n + j] = static_cast<uint8_t>((r >> (L - 1 - j)) & 1u);
 }
 
-bool crc_check(CrcKind kind, const uint8_t* bits, size_t n) {
+bool crc_check(CrcKind kind, const uint8_t* bits, size_t n, Convention conv) {
   const size_t L = static_cast<size_t>(crc_length(kind));
   if (n < L) return false;
-  const uint32_t r = crc_remainder(kind, bits, n - L);
+  const uint32_t r = crc_remainder(kind, bits, n - L, conv);
   for (size_t j = 0; j < L; ++j)
     if (((r >> (L - 1 - j)) & 1u) != (bits[n - L + j] & 1u)) return false;
   return true;
@@ -180,7 +184,8 @@ Segmentation segment_sizes(size_t b) {
   return s;
 }
 
-void segment_bits(const uint8_t* bits, size_t b, const Segmentation& s, uint8_t* out) {
+void segment_bits(const uint8_t* bits, size_t b, const Segmentation& s, uint8_t* out,
+                  Convention conv) {
   size_t cursor = 0;
   for (size_t r = 0; r < s.c; ++r) {
     const size_t kr = static_cast<size_t>(s.block_k(r));
@@ -190,7 +195,7 @@ void segment_bits(const uint8_t* bits, size_t b, const Segmentation& s, uint8_t*
     if (cursor + payload > b) throw InvalidArgument("segmentation does not match B");
     std::copy(bits + cursor, bits + cursor + payload, out + off);
     cursor += payload;
-    if (s.l == 24) crc_append(CrcKind::Crc24B, out + off, payload, out + off);
+    if (s.l == 24) crc_append(CrcKind::Crc24B, out + off, payload, out + off, conv);
     out += kr;
   }
 }
@@ -199,37 +204,50 @@ void segment_bits(const uint8_t* bits, size_t b, const Segmentation& s, uint8_t*
 // Turbo encoder
 // ------------------------------------------------------------------------------------------
 namespace {
-inline void rsc(uint8_t& state, uint8_t u, uint8_t& parity) {
+// one RSC step: the reference's feedback u^s1^s2 (lte_turbo.cpp:337) or TS 36.212's u^s0^s1
+// (g0 = 1 + D^2 + D^3); parity fb^s0^s2 (g1 = 1 + D + D^3) and next state (fb s2 s1) in both
+inline void rsc(uint8_t& state, uint8_t u, uint8_t& parity, bool std3gpp) {
   const uint8_t s0 = state & 1u, s1 = (state >> 1) & 1u, s2 = (state >> 2) & 1u;
-  const uint8_t fb = u ^ s1 ^ s2;  // reference feedback u^s1^s2 (lte_turbo.cpp:337)
+  const uint8_t fb = std3gpp ? (u ^ s0 ^ s1) : (u ^ s1 ^ s2);
   parity = fb ^ s0 ^ s2;
   state = static_cast<uint8_t>((fb << 2) | (s2 << 1) | s1);
 }
+inline uint8_t termination_input(uint8_t state, bool std3gpp) {  // the input that zeroes fb
+  return std3gpp ? ((state & 1u) ^ ((state >> 1) & 1u))
+                 : (((state >> 1) & 1u) ^ ((state >> 2) & 1u));
+}
 }  // namespace
 
-void turbo_encode(int32_t k, int32_t filler, const uint8_t* cb, uint8_t* d012) {
+void turbo_encode(int32_t k, int32_t filler, const uint8_t* cb, uint8_t* d012, Convention conv) {
+  const bool std3gpp = conv == Convention::Std3gpp;
   const auto perm = qpp_permutation(k);
   uint8_t* d0 = d012;
   uint8_t* d1 = d012 + (k + 4);
   uint8_t* d2 = d012 + 2 * (k + 4);
   uint8_t su = 0, sl = 0, p = 0;
   for (int32_t i = 0; i < k; ++i) {
-    rsc(su, cb[i] & 1u, p);
+    rsc(su, cb[i] & 1u, p, std3gpp);
     d0[i] = (i < filler) ? 0 : (cb[i] & 1u);
     d1[i] = (i < filler) ? 0 : p;
-    rsc(sl, cb[perm[i]] & 1u, p);
+    rsc(sl, cb[perm[i]] & 1u, p, std3gpp);
     d2[i] = p;
   }
   uint8_t us[3], up[3], ls[3], lp[3];
   for (int i = 0; i < 3; ++i) {
-    us[i] = ((su >> 1) & 1u) ^ ((su >> 2) & 1u);  // input that zeroes the feedback
-    rsc(su, us[i], up[i]);
-    ls[i] = ((sl >> 1) & 1u) ^ ((sl >> 2) & 1u);
-    rsc(sl, ls[i], lp[i]);
+    us[i] = termination_input(su, std3gpp);
+    rsc(su, us[i], up[i], std3gpp);
+    ls[i] = termination_input(sl, std3gpp);
+    rsc(sl, ls[i], lp[i], std3gpp);
   }
-  d0[k] = us[0]; d0[k + 1] = up[1]; d0[k + 2] = us[1]; d0[k + 3] = up[2];
-  d1[k] = up[0]; d1[k + 1] = us[1]; d1[k + 2] = up[2]; d1[k + 3] = ls[0];
-  d2[k] = lp[0]; d2[k + 1] = ls[1]; d2[k + 2] = lp[1]; d2[k + 3] = ls[2];
+  if (!std3gpp) {  // the reference's multiplexing (lte_turbo.cpp:664-677)
+    d0[k] = us[0]; d0[k + 1] = up[1]; d0[k + 2] = us[1]; d0[k + 3] = up[2];
+    d1[k] = up[0]; d1[k + 1] = us[1]; d1[k + 2] = up[2]; d1[k + 3] = ls[0];
+    d2[k] = lp[0]; d2[k + 1] = ls[1]; d2[k + 2] = lp[1]; d2[k + 3] = ls[2];
+  } else {  // TS 36.212 5.1.3.2.2: x_K z_K+1 x'_K z'_K+1 / z_K x_K+2 z'_K x'_K+2 / x_K+1 z_K+2 x'_K+1 z'_K+2
+    d0[k] = us[0]; d0[k + 1] = up[1]; d0[k + 2] = ls[0]; d0[k + 3] = lp[1];
+    d1[k] = up[0]; d1[k + 1] = us[2]; d1[k + 2] = lp[0]; d1[k + 3] = ls[2];
+    d2[k] = us[1]; d2[k + 1] = up[2]; d2[k + 2] = ls[1]; d2[k + 3] = lp[2];
+  }
 }
 
 // ------------------------------------------------------------------------------------------

@@ -19,15 +19,25 @@ int qpp_index(int32_t k);  // -1 if K is not an LTE turbo block size
 std::vector<int32_t> qpp_permutation(int32_t k);          // Pi(i) = (f1 i + f2 i^2) mod K
 std::vector<int32_t> qpp_inverse_permutation(int32_t k);
 
+// ---- code conventions ----
+// Reference: the conventions of the reference (its CRC coefficient arrays, RSC feedback
+// u^s1^s2, its tail multiplexing) -- the default everywhere, and what parity is judged on.
+// Std3gpp: TS 36.212 (CRC generators gCRC24A/24B/16/8 of 5.1.1, RSC feedback g0 = 1+D^2+D^3 and
+// the tail multiplexing of 5.1.3.2.2).  Segmentation and rate matching do not depend on it.
+enum class Convention : int { Reference = 0, Std3gpp = 1 };
+
 // ---- CRC (lte_turbo.cpp:104-155, 508-538) ----
-// The generators are the reference's coefficient arrays (g[j] multiplies D^(L-1-j), leading
-// D^L implicit); they are not all the TS 36.212 polynomials.
+// Reference generators are the reference's coefficient arrays (g[j] multiplies D^(L-1-j),
+// leading D^L implicit); they are not all the TS 36.212 polynomials.
 enum class CrcKind : int { Crc24A = 0, Crc24B = 1, Crc16 = 2, Crc8 = 3 };
 int crc_length(CrcKind kind);
-uint32_t crc_generator_mask(CrcKind kind);  // bit (L-1-j) = g[j]
-uint32_t crc_remainder(CrcKind kind, const uint8_t* bits, size_t n);  // M(D) D^L mod g(D)
-void crc_append(CrcKind kind, const uint8_t* bits, size_t n, uint8_t* out);  // out: n+L bits
-bool crc_check(CrcKind kind, const uint8_t* bits, size_t n);
+uint32_t crc_generator_mask(CrcKind kind, Convention conv = Convention::Reference);
+uint32_t crc_remainder(CrcKind kind, const uint8_t* bits, size_t n,
+                       Convention conv = Convention::Reference);  // M(D) D^L mod g(D)
+void crc_append(CrcKind kind, const uint8_t* bits, size_t n, uint8_t* out,
+                Convention conv = Convention::Reference);  // out: n+L bits
+bool crc_check(CrcKind kind, const uint8_t* bits, size_t n,
+               Convention conv = Convention::Reference);
 
 // ---- code-block segmentation (lte_turbo.cpp:540-604) ----
 struct Segmentation {
@@ -38,12 +48,14 @@ struct Segmentation {
 Segmentation segment_sizes(size_t b);  // throws InvalidArgument / std::runtime_error
 // Writes the C code blocks back to back (filler zeros first in block 0, CRC24B per block when
 // C > 1).
-void segment_bits(const uint8_t* bits_with_crc, size_t b, const Segmentation& s, uint8_t* out);
+void segment_bits(const uint8_t* bits_with_crc, size_t b, const Segmentation& s, uint8_t* out,
+                  Convention conv = Convention::Reference);
 
 // ---- turbo encoder (lte_turbo.cpp:333-353, 624-688) ----
 // d012 = [d0 | d1 | d2], each K+4 bits; filler positions of d0/d1 are 0; tails multiplexed as
-// the reference does (lte_turbo.cpp:664-677).
-void turbo_encode(int32_t k, int32_t filler, const uint8_t* cb_bits, uint8_t* d012);
+// the reference does (lte_turbo.cpp:664-677), or as TS 36.212 5.1.3.2.2 with Std3gpp.
+void turbo_encode(int32_t k, int32_t filler, const uint8_t* cb_bits, uint8_t* d012,
+                  Convention conv = Convention::Reference);
 
 // ---- rate matching (lte_turbo.cpp:167-325) ----
 size_t compute_e(size_t r, size_t g_total, size_t c, size_t num_layers, size_t mod_order);

@@ -123,11 +123,21 @@ struct CkptGlobal {
   }
 };
 
-// Tail LLRs in the reference's decoder mapping (lte_turbo.cpp:758-773).
+// Tail LLRs in the reference's decoder mapping (lte_turbo.cpp:758-773), or (STD) in the
+// inverse of TS 36.212 5.1.3.2.2's multiplexing: upper systematic x_K..x_K+2 = d0[K], d2[K],
+// d1[K+1], parity z_K..z_K+2 = d1[K], d0[K+1], d2[K+1]; lower x' = d0[K+2], d2[K+2], d1[K+3],
+// z' = d1[K+2], d0[K+3], d2[K+3].
+template <bool STD = false>
 __device__ __forceinline__ void tail_llrs(bool lower, const float* d0, int k, float ts[3],
                                           float tp[3]) {
   const float* d1 = d0 + (k + 4);
   const float* d2 = d1 + (k + 4);
+  if (STD) {
+    const int o = lower ? 2 : 0;
+    ts[0] = d0[k + o]; ts[1] = d2[k + o]; ts[2] = d1[k + o + 1];
+    tp[0] = d1[k + o]; tp[1] = d0[k + o + 1]; tp[2] = d2[k + o + 1];
+    return;
+  }
   if (!lower) {
     ts[0] = d0[k]; ts[1] = d0[k + 2]; ts[2] = 0.0f;
     tp[0] = d1[k]; tp[1] = d0[k + 1]; tp[2] = d1[k + 2];
@@ -143,7 +153,7 @@ __device__ __forceinline__ void tail_llrs(bool lower, const float* d0, int k, fl
 // kernels, one specialisation each) or run-time values (the persistent kernel, which keeps a
 // single copy of this code for both halves).  COHERENT: a-priori and seeds were written earlier
 // in the same kernel (persistent schedule).
-template <int S, class Ckpt, bool COHERENT>
+template <int S, class Ckpt, bool COHERENT, bool STD = false>
 __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, const SisoIo& io,
                                                const Ckpt& ck, const bool LOWER, const bool POST) {
   static_assert(S == 4, "sub-windows are one float4 group of 4 steps");
@@ -174,11 +184,11 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
       if (q >= lo) ck.store((q - lo) / S, al);
       scale4(cur.lo, sa, a, b);
 #pragma unroll
-      for (int t = 0; t < 4; ++t) alpha_step(al, a[t], b[t]);
+      for (int t = 0; t < 4; ++t) alpha_step<STD>(al, a[t], b[t]);
       if (q >= lo) ck.store((q - lo) / S + 1, al);
       scale4(cur.hi, sa, a, b);
 #pragma unroll
-      for (int t = 0; t < 4; ++t) alpha_step(al, a[t], b[t]);
+      for (int t = 0; t < 4; ++t) alpha_step<STD>(al, a[t], b[t]);
       cur = nxt;
     }
   }
@@ -202,8 +212,8 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
   if (b_hi >= K) {
     b_hi = K;
     float ts[3], tp[3];
-    tail_llrs(LOWER, d0, K, ts, tp);
-    tail_beta(be, ts, tp);
+    tail_llrs<STD>(LOWER, d0, K, ts, tp);
+    tail_beta<STD>(be, ts, tp);
   } else {
     const float4 x = ld4_io<COHERENT>(io.seed_in + 16 * g + 8), y = ld4_io<COHERENT>(io.seed_in + 16 * g + 12);
     be[0] = x.x; be[1] = x.y; be[2] = x.z; be[3] = x.w; be[4] = y.x; be[5] = y.y; be[6] = y.z; be[7] = y.w;
@@ -215,10 +225,10 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
       if (q - 8 >= hi) nxt = load_raw8<COHERENT>(sys, apr, par, q - 8);
       scale4(cur.hi, sa, a, b);
 #pragma unroll
-      for (int t = 3; t >= 0; --t) beta_step(be, a[t], b[t]);
+      for (int t = 3; t >= 0; --t) beta_step<STD>(be, a[t], b[t]);
       scale4(cur.lo, sa, a, b);
 #pragma unroll
-      for (int t = 3; t >= 0; --t) beta_step(be, a[t], b[t]);
+      for (int t = 3; t >= 0; --t) beta_step<STD>(be, a[t], b[t]);
       cur = nxt;
     }
   }
@@ -260,16 +270,16 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
     for (int t = 0; t + 1 < S; ++t) {
 #pragma unroll
       for (int s = 0; s < 8; ++s) Al[t + 1][s] = Al[t][s];
-      alpha_step(Al[t + 1], A_[t], B_[t]);
+      alpha_step<STD>(Al[t + 1], A_[t], B_[t]);
     }
     const uint32_t w2[2] = {iv.x, iv.y};
 #pragma unroll
     for (int t = S - 1; t >= 0; --t) {
-      const float e = io.scale * (kLn2 * extrinsic2(Al[t], be, B_[t]));
+      const float e = io.scale * (kLn2 * extrinsic2<STD>(Al[t], be, B_[t]));
       const int n = static_cast<int>((w2[t >> 1] >> (16 * (t & 1))) & 0xffffu);
       io.ext[cb.work + n] = e;
       if (POST) io.post[cb.out + n] = SA[t] + e;
-      beta_step(be, A_[t], B_[t]);
+      beta_step<STD>(be, A_[t], B_[t]);
       if (rec_beta && base + t == lo + G) {
         bseed[0] = make_float4(be[0], be[1], be[2], be[3]);
         bseed[1] = make_float4(be[4], be[5], be[6], be[7]);
@@ -278,10 +288,10 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
   }
 }
 
-template <int S, bool LOWER, bool POST, class Ckpt, bool COHERENT = false>
+template <int S, bool LOWER, bool POST, class Ckpt, bool COHERENT = false, bool STD = false>
 __device__ __forceinline__ void siso_window(const DevCb& cb, int w, int g, const SisoIo& io,
                                             const Ckpt& ck) {
-  siso_window_rt<S, Ckpt, COHERENT>(cb, w, g, io, ck, LOWER, POST);
+  siso_window_rt<S, Ckpt, COHERENT, STD>(cb, w, g, io, ck, LOWER, POST);
 }
 
 }  // namespace tcb

@@ -6,10 +6,13 @@
 // of the reference, 0.5 * (+-(Ls+La) +- Lp) (lte_turbo.cpp:437-438), becomes +-a +-b with
 // a = 0.5*log2(e)*(Ls+La) and b = 0.5*log2(e)*Lp.
 //
-// Trellis (lte_turbo.cpp:333-341): state = (s2 s1 s0), feedback fb = u^s1^s2, parity
-// fb^s0^s2, next state (fb s2 s1).  Hence next state n = (n2 n1 n0) is reached with input
-// u = n2^n1^n0 from the two predecessors 2*(n&3) + s0, s0 in {0,1}, whose parities are
-// n2^n1^s0.  All state/branch indexing below is resolved at compile time.
+// Trellis (lte_turbo.cpp:333-341): state = (s2 s1 s0), s2 the newest register, feedback
+// fb = u^s1^s2, parity fb^s0^s2, next state (fb s2 s1).  Hence next state n = (n2 n1 n0) is
+// reached from the two predecessors 2*(n&3) + x, x in {0,1}, with input u = n2^n1^n0 and
+// parities n2^n1^x.  The TS 36.212 code (template flag STD; not the reference's convention)
+// feeds back the two oldest registers, fb = u^s0^s1 (g0 = 1 + D^2 + D^3); its parity is the
+// same fb^s0^s2 and its next state the same (fb s2 s1), so only the inputs change: predecessor
+// x reaches n with u = n2^n0^x.  All state/branch indexing below is resolved at compile time.
 #pragma once
 #include <cstdint>
 
@@ -40,11 +43,30 @@ __device__ __forceinline__ float max_star(float x, float y) {
   return m + lg2(1.0f + ex2(-d));
 }
 
-__host__ __device__ constexpr int next_state(int s, int u) {
-  return ((u ^ ((s >> 1) & 1) ^ ((s >> 2) & 1)) << 2) | (((s >> 2) & 1) << 1) | ((s >> 1) & 1);
+template <bool STD = false>
+__host__ __device__ constexpr int feedback(int s, int u) {
+  return STD ? (u ^ (s & 1) ^ ((s >> 1) & 1)) : (u ^ ((s >> 1) & 1) ^ ((s >> 2) & 1));
 }
+template <bool STD = false>
+__host__ __device__ constexpr int next_state(int s, int u) {
+  return (feedback<STD>(s, u) << 2) | (((s >> 2) & 1) << 1) | ((s >> 1) & 1);
+}
+template <bool STD = false>
 __host__ __device__ constexpr int parity(int s, int u) {
-  return (u ^ ((s >> 1) & 1) ^ ((s >> 2) & 1)) ^ (s & 1) ^ ((s >> 2) & 1);
+  return feedback<STD>(s, u) ^ (s & 1) ^ ((s >> 2) & 1);
+}
+// the termination input of state s: the one that makes the feedback 0
+template <bool STD = false>
+__host__ __device__ constexpr int termination_input(int s) {
+  return STD ? ((s & 1) ^ ((s >> 1) & 1)) : (((s >> 1) & 1) ^ ((s >> 2) & 1));
+}
+// input and parity of the branch from predecessor 2*(n&3) + x into next state n
+template <bool STD = false>
+__host__ __device__ constexpr int pred_input(int n, int x) {
+  return STD ? (((n >> 2) & 1) ^ (n & 1) ^ x) : (((n >> 2) & 1) ^ ((n >> 1) & 1) ^ (n & 1));
+}
+__host__ __device__ constexpr int pred_parity(int n, int x) {
+  return ((n >> 2) & 1) ^ ((n >> 1) & 1) ^ x;
 }
 // branch metric +-a +-b for input u and parity p: g0 = a+b, g1 = a-b
 __device__ __forceinline__ float branch(int u, int p, float g0, float g1) {
@@ -52,16 +74,15 @@ __device__ __forceinline__ float branch(int u, int p, float g0, float g1) {
 }
 
 // alpha_{t+1} from alpha_t (in place); normalised so that state 0 is 0.
+template <bool STD = false>
 __device__ __forceinline__ void alpha_step(float (&al)[8], float a, float b) {
   const float g0 = a + b, g1 = a - b;
   float an[8];
 #pragma unroll
   for (int n = 0; n < 8; ++n) {
-    const int n2 = (n >> 2) & 1, n1 = (n >> 1) & 1, n0 = n & 1;
-    const int u = n2 ^ n1 ^ n0;
     const int p0 = 2 * (n & 3);
-    an[n] = max_star(al[p0] + branch(u, n2 ^ n1, g0, g1),
-                     al[p0 + 1] + branch(u, n2 ^ n1 ^ 1, g0, g1));
+    an[n] = max_star(al[p0] + branch(pred_input<STD>(n, 0), pred_parity(n, 0), g0, g1),
+                     al[p0 + 1] + branch(pred_input<STD>(n, 1), pred_parity(n, 1), g0, g1));
   }
   const float r = an[0];
   al[0] = 0.0f;  // an[0] - an[0]
@@ -70,13 +91,14 @@ __device__ __forceinline__ void alpha_step(float (&al)[8], float a, float b) {
 }
 
 // beta_t from beta_{t+1} (in place); normalised so that state 0 is 0.
+template <bool STD = false>
 __device__ __forceinline__ void beta_step(float (&be)[8], float a, float b) {
   const float g0 = a + b, g1 = a - b;
   float bn[8];
 #pragma unroll
   for (int s = 0; s < 8; ++s)
-    bn[s] = max_star(be[next_state(s, 0)] + branch(0, parity(s, 0), g0, g1),
-                     be[next_state(s, 1)] + branch(1, parity(s, 1), g0, g1));
+    bn[s] = max_star(be[next_state<STD>(s, 0)] + branch(0, parity<STD>(s, 0), g0, g1),
+                     be[next_state<STD>(s, 1)] + branch(1, parity<STD>(s, 1), g0, g1));
   const float r = bn[0];
   be[0] = 0.0f;  // bn[0] - bn[0]
 #pragma unroll
@@ -87,12 +109,13 @@ __device__ __forceinline__ void beta_step(float (&be)[8], float a, float b) {
 // u=0 branches of alpha_t + beta_{t+1} +- b.  The +-a part is common to each side and is the
 // (Ls+La) term the reference subtracts again (lte_turbo.cpp:483), so it is left out.
 // Each 8-way log-sum is max + lg2(sum 2^(m - max)): 8 ex2 + 1 lg2 instead of 7 pairwise max*.
+template <bool STD = false>
 __device__ __forceinline__ float extrinsic2(const float (&al)[8], const float (&be)[8], float b) {
   float m0[8], m1[8];
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
-    m0[s] = al[s] + be[next_state(s, 0)] + (parity(s, 0) ? b : -b);
-    m1[s] = al[s] + be[next_state(s, 1)] + (parity(s, 1) ? b : -b);
+    m0[s] = al[s] + be[next_state<STD>(s, 0)] + (parity<STD>(s, 0) ? b : -b);
+    m1[s] = al[s] + be[next_state<STD>(s, 1)] + (parity<STD>(s, 1) ? b : -b);
   }
   float x0 = fmaxf(fmaxf(fmaxf(m0[0], m0[1]), fmaxf(m0[2], m0[3])),
                    fmaxf(fmaxf(m0[4], m0[5]), fmaxf(m0[6], m0[7])));
@@ -108,8 +131,9 @@ __device__ __forceinline__ float extrinsic2(const float (&al)[8], const float (&
 }
 
 // beta at the block end from the three termination steps (lte_turbo.cpp:343-378): from each
-// state the tail input is s1^s2 (feedback 0), which drives every state to 0 in three steps.
-// ts/tp are the tail systematic / parity LLRs in the reference's mapping.
+// state the tail input is the one that zeroes the feedback, which drives every state to 0 in
+// three steps.  ts/tp are the tail systematic / parity LLRs of this SISO.
+template <bool STD = false>
 __device__ __forceinline__ void tail_beta(float (&be)[8], const float ts[3], const float tp[3]) {
 #pragma unroll
   for (int s0 = 0; s0 < 8; ++s0) {
@@ -117,10 +141,10 @@ __device__ __forceinline__ void tail_beta(float (&be)[8], const float ts[3], con
     float m = 0.0f;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      const int u = ((s >> 1) & 1) ^ ((s >> 2) & 1);
-      const int p = parity(s, u);
+      const int u = termination_input<STD>(s);
+      const int p = parity<STD>(s, u);
       m += (u ? ts[i] : -ts[i]) + (p ? tp[i] : -tp[i]);
-      s = next_state(s, u);
+      s = next_state<STD>(s, u);
     }
     be[s0] = m * kHalfLog2e;
   }
