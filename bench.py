@@ -181,10 +181,10 @@ def ncu_traffic(schedule: str):
 
 
 # ------------------------------------------------------------------------------------------
-def cpu_reference_sample(tc, seconds: float, threads: int = 0):
-    """The reference decoder (oracle/_ref, else the oracle port) over a bounded sample of the
-    same workload on all host cores.  Returns (Mbit/s, cores, kind, sample description, bits,
-    posterior)."""
+def reference_sample(tc, seconds: float, threads: int = 0):
+    """A bounded sample of the workload for the reference decoder (oracle/_ref, else the oracle
+    port) on all host cores, sized to ~`seconds` of wall time.  Returns (decoder library, kind,
+    cores, n, bits, llr, Eb/N0 per block)."""
     import oracle
 
     cores = threads or os.cpu_count() or 1
@@ -202,28 +202,45 @@ def cpu_reference_sample(tc, seconds: float, threads: int = 0):
     n = max(cores, (n // cores) * cores)
     eb = np.array([EBN0[i % len(EBN0)] for i in range(n)], np.float32)
     bits, llr = tc.awgn_code_blocks(78, [K] * n, eb)
+    return lib, kind, cores, n, bits, llr, eb
+
+
+def time_reference(lib, cores, n, llr):
+    """One timed decode of the sample: (Mbit/s, posterior)."""
     lo = np.arange(n, dtype=np.int64) * 3 * (K + 4)
     oo = np.arange(n, dtype=np.int64) * K
     t = time.perf_counter()
     post, _, _ = lib.decode_batch(np.full(n, K, np.int32), np.zeros(n, np.int32), llr, lo, oo, 8,
                                   threads=cores)
-    dt = time.perf_counter() - t
-    sample = (f"{n} code blocks of K=6144 (Eb/N0 0.0..1.2 dB cycled), 8 iterations, one block "
-              f"per task on {cores} threads ({kind})")
-    return n * K / dt / 1e6, cores, kind, sample, bits, post, eb
+    return n * K / (time.perf_counter() - t) / 1e6, post
+
+
+def sample_text(n, cores, kind):
+    return (f"{n} code blocks of K=6144 (Eb/N0 0.0..1.2 dB cycled), 8 iterations, one block "
+            f"per task on {cores} threads ({kind})")
+
+
+def cpu_reference_sample(tc, seconds: float, threads: int = 0):
+    """The reference decoder over a bounded sample of the same workload on all host cores.
+    Returns (Mbit/s, cores, kind, sample description, bits, posterior, Eb/N0 per block)."""
+    lib, kind, cores, n, bits, llr, eb = reference_sample(tc, seconds, threads)
+    mbps, post = time_reference(lib, cores, n, llr)
+    return mbps, cores, kind, sample_text(n, cores, kind), bits, post, eb
 
 
 def run_reference(args, world, rank):
-    """--impl reference: the reference CPU decoder on the host cores, rank 0 only."""
+    """--impl reference: the reference CPU decoder on the host cores, rank 0 only.  The sample
+    is generated once; each step decodes it, sized so that all warm-up and timed steps together
+    take about 150 s of decoding (at most 4 s per step)."""
     if rank != 0:
         return
     import turbo_cpp_b200 as tc
 
+    per_step = min(4.0, max(0.25, 150.0 / max(1, args.warmup + args.steps)))
+    lib, kind, cores, n, _, llr, _ = reference_sample(tc, per_step)
     steps = []
-    cores = os.cpu_count() or 1
     for i in range(args.warmup + args.steps):
-        mbps, cores, kind, sample, _, _, _ = cpu_reference_sample(
-            tc, max(2.0, args.cpu_seconds / 3), cores)
+        mbps, _ = time_reference(lib, cores, n, llr)
         if i >= args.warmup:
             steps.append(mbps)
     v = float(np.mean(steps))
@@ -234,7 +251,7 @@ def run_reference(args, world, rank):
         "data": "synthetic: seeded uniform info bits, BPSK/AWGN, Eb/N0 0.0..1.2 dB, FP32 LLRs",
         "config": workload_config(args), "impl": "reference",
         "cpu_baseline": {"value": v, "unit": "Mbit/s", "cores": cores, "kind": kind,
-                         "sample": sample + "; each step one such sample"},
+                         "sample": sample_text(n, cores, kind) + "; each step decodes it once"},
         "e2e": {"value": v, "unit": "Mbit/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
