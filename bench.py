@@ -12,7 +12,8 @@ Lines printed by rank 0 (one JSON object):
                max over ranks, whole-job aggregate (weak scaling: every rank decodes its own
                batches, code blocks are independent, no collective on the data path)
   e2e       -- the same metric through the C ABI with pinned host buffers: H2D of the LLRs,
-               decode, D2H of posterior/flags inside the timed region (tc_decode, TC_MEM_HOST)
+               decode, D2H of posterior/flags inside the timed region (back-to-back
+               tc_decode calls with TC_MEM_HOST_ASYNC; e2e.synchronous: TC_MEM_HOST calls)
   roofline  -- dominant kernel (SISO half-iteration) against the SFU (MUFU) issue roofline
   roofline_hbm -- the same kernel's algorithmic bytes against measured HBM bandwidth
   cpu_baseline -- the reference CPU decoder (oracle/_ref) on all host cores, bounded sample
@@ -38,7 +39,7 @@ sys.path.insert(0, ROOT)
 METRIC = "info Mbit/s @8 iters, matched BLER: batched vs plain GPU vs CPU ref; adjoint err"
 EBN0 = [0.0, 0.2, 0.4, 0.6, 0.8, 1.0, 1.2]
 K = 6144
-# SURVEY-d algorithmic work of one trellis step of one SISO: 30 max*, 2 transcendentals each
+# algorithmic work of one trellis step of one SISO: 30 max*, 2 transcendentals each
 TRANSC_PER_STEP = 60
 # algorithmic HBM bytes per info bit of a whole decode: 3(K+4) LLRs in + K posteriors out
 BYTES_PER_BIT = 4.0 * (3 * (K + 4) + K) / K
@@ -184,7 +185,7 @@ def ncu_traffic(schedule: str):
 def reference_sample(tc, seconds: float, threads: int = 0):
     """A bounded sample of the workload for the reference decoder (oracle/_ref, else the oracle
     port) on all host cores, sized to ~`seconds` of wall time.  Returns (decoder library, kind,
-    cores, n, bits, llr, Eb/N0 per block)."""
+    cores, n, bits, llr, Eb/N0 per block, single-thread Mbit/s of the sizing probe)."""
     import oracle
 
     cores = threads or os.cpu_count() or 1
@@ -202,7 +203,7 @@ def reference_sample(tc, seconds: float, threads: int = 0):
     n = max(cores, (n // cores) * cores)
     eb = np.array([EBN0[i % len(EBN0)] for i in range(n)], np.float32)
     bits, llr = tc.awgn_code_blocks(78, [K] * n, eb)
-    return lib, kind, cores, n, bits, llr, eb
+    return lib, kind, cores, n, bits, llr, eb, K / per_cb / 1e6
 
 
 def time_reference(lib, cores, n, llr):
@@ -222,10 +223,11 @@ def sample_text(n, cores, kind):
 
 def cpu_reference_sample(tc, seconds: float, threads: int = 0):
     """The reference decoder over a bounded sample of the same workload on all host cores.
-    Returns (Mbit/s, cores, kind, sample description, bits, posterior, Eb/N0 per block)."""
-    lib, kind, cores, n, bits, llr, eb = reference_sample(tc, seconds, threads)
+    Returns (Mbit/s, cores, kind, sample description, bits, posterior, Eb/N0 per block,
+    single-thread Mbit/s)."""
+    lib, kind, cores, n, bits, llr, eb, one = reference_sample(tc, seconds, threads)
     mbps, post = time_reference(lib, cores, n, llr)
-    return mbps, cores, kind, sample_text(n, cores, kind), bits, post, eb
+    return mbps, cores, kind, sample_text(n, cores, kind), bits, post, eb, one
 
 
 def run_reference(args, world, rank):
@@ -237,7 +239,7 @@ def run_reference(args, world, rank):
     import turbo_cpp_b200 as tc
 
     per_step = min(4.0, max(0.25, 150.0 / max(1, args.warmup + args.steps)))
-    lib, kind, cores, n, _, llr, _ = reference_sample(tc, per_step)
+    lib, kind, cores, n, _, llr, _, one = reference_sample(tc, per_step)
     steps = []
     for i in range(args.warmup + args.steps):
         mbps, _ = time_reference(lib, cores, n, llr)
@@ -251,7 +253,8 @@ def run_reference(args, world, rank):
         "data": "synthetic: seeded uniform info bits, BPSK/AWGN, Eb/N0 0.0..1.2 dB, FP32 LLRs",
         "config": workload_config(args), "impl": "reference",
         "cpu_baseline": {"value": v, "unit": "Mbit/s", "cores": cores, "kind": kind,
-                         "sample": sample_text(n, cores, kind) + "; each step decodes it once"},
+                         "sample": sample_text(n, cores, kind) + "; each step decodes it once",
+                         "single_thread_value": one},
         "e2e": {"value": v, "unit": "Mbit/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -725,10 +728,11 @@ def main():
                                       "per synchronous call, host buffers, 8 blocks"}
     line["batched_vs_plain_per_block"] = value / line["plain_per_block"]["value"]
     if rank == 0 and not args.no_cpu:
-        mbps, cores, kind, sample, cbits, cpost, ceb = cpu_reference_sample(tc, args.cpu_seconds)
+        mbps, cores, kind, sample, cbits, cpost, ceb, one = cpu_reference_sample(tc, args.cpu_seconds)
         cn = cbits.size // K
         line["cpu_baseline"] = {"value": mbps, "unit": "Mbit/s", "cores": cores, "kind": kind,
-                                "sample": sample}
+                                "sample": sample, "single_thread_value": one,
+                                "single_thread_sample": "one K=6144 block at 0.6 dB, 8 iterations"}
         line["cpu_ber_bler"] = [
             {"ebn0_db": float(e), "blocks": int((ceb == e).sum()),
              "ber": float(((cpost >= 0) != cbits).reshape(cn, K)[ceb == e].mean()),

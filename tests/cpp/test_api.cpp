@@ -211,7 +211,7 @@ double rel_err(const std::vector<float>& got, const std::vector<float>& ref) {
 }
 
 // The reference's round-trip cases (test_main.cpp) through every GPU backend, with the CPU
-// decoder's posterior as the judge.
+// decoder's posterior as the reference.
 void roundtrip_case(std::size_t tbs, std::size_t a, std::size_t c, bool g_from_blocks,
                     std::size_t g_total) {
   tb::LteTurboCodecParams p;
@@ -263,7 +263,7 @@ void roundtrip_case(std::size_t tbs, std::size_t a, std::size_t c, bool g_from_b
   expect(hard && it == 6, "tile8 hard decisions");
 }
 
-// A transport block of the 36.212 code through the GPU backends, judged by the oracle's 36.212
+// A transport block of the 36.212 code through the GPU backends, checked against the oracle's 36.212
 // restatement on the full trellis.
 void std3gpp_roundtrip_case(std::size_t tbs) {
   tb::LteTurboCodecParams p;

@@ -179,3 +179,44 @@ def test_graph_on_the_legacy_stream_is_refused(tc, decoder):
                           options=opts, stream=s.cuda_stream)
     s.synchronize()
     assert np.array_equal(p.cpu().numpy(), ref)
+
+
+def test_std_async_host_calls_and_autotuned_schedule(tc):
+    """TC_MEM_HOST_ASYNC and the autotuner carry the convention: asynchronous calls equal the
+    synchronous ones, and SCHEDULE_AUTO after tuning a 36.212 request decodes the 36.212 code."""
+    import torch
+
+    dec = tc.Decoder(0)
+    ks = [6144] * 64 + [1056] * 32 + [40] * 8
+    cbs, llr_len, post_len = tc.Decoder.layout(ks)
+    conv = tc.CONVENTION_3GPP
+    o = tc.DecodeOptions(8, True, schedule=tc.SCHEDULE_PERSISTENT, convention=conv)
+    calls = []
+    for i in range(3):
+        llr, _ = std_code_blocks(tc, ks, 0.6 + 0.3 * i, seed=40 + i)
+        x = torch.from_numpy(llr).pin_memory()
+        p = torch.zeros(post_len).pin_memory()
+        c = torch.zeros(len(ks), dtype=torch.uint8).pin_memory()
+        it = torch.zeros(len(ks), dtype=torch.int32).pin_memory()
+        dec.decode_async(cbs, len(ks), x.data_ptr(), llr_len, p.data_ptr(), post_len,
+                         c.data_ptr(), it.data_ptr(), options=o)
+        calls.append((llr, p, c, it))
+    dec.sync()
+    for llr, p, c, it in calls:
+        post, ok, used = dec.decode(ks, llr, options=o)
+        assert np.array_equal(p.numpy(), post)
+        assert np.array_equal(c.numpy().astype(bool), ok)
+        assert np.array_equal(it.numpy().astype(np.uint32), used)
+
+    llr, cb_bits = std_code_blocks(tc, ks, 3.0, seed=45)
+    x = torch.from_numpy(llr).cuda()
+    out = torch.zeros(post_len, device="cuda")
+    s = torch.cuda.Stream()
+    best = dec.autotune(cbs, len(ks), x.data_ptr(), llr_len, out.data_ptr(), post_len,
+                        options=tc.DecodeOptions(8, convention=conv), stream=s.cuda_stream)
+    assert best["schedule"] in (0, 1) and best["ms"] > 0
+    dec.decode_device(cbs, len(ks), x.data_ptr(), llr_len, out.data_ptr(), post_len,
+                      options=tc.DecodeOptions(8, schedule=tc.SCHEDULE_AUTO, convention=conv),
+                      stream=s.cuda_stream)
+    s.synchronize()
+    assert np.array_equal((out.cpu().numpy() >= 0).astype(np.uint8), np.concatenate(cb_bits))

@@ -21,7 +21,7 @@ std::vector<int32_t> qpp_inverse_permutation(int32_t k);
 
 // ---- code conventions ----
 // Reference: the conventions of the reference (its CRC coefficient arrays, RSC feedback
-// u^s1^s2, its tail multiplexing) -- the default everywhere, and what parity is judged on.
+// u^s1^s2, its tail multiplexing) -- the default everywhere, and what parity is checked against.
 // Std3gpp: TS 36.212 (CRC generators gCRC24A/24B/16/8 of 5.1.1, RSC feedback g0 = 1+D^2+D^3 and
 // the tail multiplexing of 5.1.3.2.2).  Segmentation and rate matching do not depend on it.
 enum class Convention : int { Reference = 0, Std3gpp = 1 };
