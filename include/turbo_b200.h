@@ -253,7 +253,10 @@ TC_API int tc_derate_combine_llr_device(tc_decoder* dec, size_t n_tx, const tc_r
  * and CRC24A.  The code blocks of transport block t are cbs[first_cb .. first_cb + n_cb); their
  * llr_offset is ignored.  tb_bits receives one byte (0/1) per decoded bit at bits_offset;
  * tb_crc_ok (n_tb), cb_crc_ok, iterations_used (n_cb) and posterior (sum K, may be NULL) follow
- * opts->memory like the rate-matched LLRs. */
+ * opts->memory like the rate-matched LLRs.  TC_MEM_HOST_ASYNC (new): host pointers; the call
+ * is enqueued on one of the decoder's three worker workspaces and returns, so that one call's
+ * copies overlap earlier calls' decoding; results are valid, and the inputs may be reused,
+ * after tc_decoder_sync (pinned buffers for the overlap). */
 typedef struct {
   int64_t tbs;         /* transport block size, without CRC24A */
   int32_t first_cb;

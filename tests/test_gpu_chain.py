@@ -115,3 +115,36 @@ def test_harq_combining_matches_host_derate_sums(tc, decoder):
         k0, f0 = tx[0][0], tx[0][1]
         bad = [tx[0], (k0, (f0 + 8) % k0) + tx[0][2:]]
         decoder.derate_combine_device(bad, e_llr.data_ptr(), e_llr.numel(), out.data_ptr(), llr_off)
+
+
+@pytest.mark.parametrize("schedule", ["plain", "persistent"])
+def test_transport_blocks_async_host_calls(tc, schedule):
+    """TC_MEM_HOST_ASYNC transport-block calls (enqueued on the worker workspaces, several in
+    flight) give the synchronous call's bits, CRC flags and iterations once synchronised."""
+    import torch
+    from turbo_cpp_b200.workloads import config3_transport_blocks
+
+    dec = tc.Decoder(0)
+    sched = tc.SCHEDULE_PLAIN if schedule == "plain" else tc.SCHEDULE_PERSISTENT
+    o = tc.DecodeOptions(8, True, 0, -1, sched)
+    calls = []
+    for i in range(4):
+        tbs, blocks, e_llr, truth, _ = config3_transport_blocks(12, seed=60 + i)
+        tba, nbits = tc.Decoder.tb_descriptors(tbs)
+        arr, e_len, _ = tc.Decoder.rm_blocks(blocks)
+        x = torch.from_numpy(np.ascontiguousarray(e_llr, np.float32)).pin_memory()
+        bits = torch.zeros(nbits, dtype=torch.uint8).pin_memory()
+        tb_ok = torch.zeros(len(tbs), dtype=torch.uint8).pin_memory()
+        cb_ok = torch.zeros(len(blocks), dtype=torch.uint8).pin_memory()
+        it = torch.zeros(len(blocks), dtype=torch.int32).pin_memory()
+        dec.decode_tbs_async(tba, len(tbs), arr, len(blocks), e_len, x.data_ptr(), nbits,
+                             bits.data_ptr(), tb_ok.data_ptr(), cb_ok.data_ptr(), it.data_ptr(),
+                             options=o)
+        calls.append((tbs, blocks, e_llr, tba, arr, x, bits, tb_ok, cb_ok, it))
+    dec.sync()
+    for tbs, blocks, e_llr, tba, arr, x, bits, tb_ok, cb_ok, it in calls:
+        ref_bits, ref_tb, ref_cb, ref_it = dec.decode_tbs(tbs, blocks, e_llr, o)
+        assert np.array_equal(bits.numpy(), np.concatenate(ref_bits))
+        assert np.array_equal(tb_ok.numpy().astype(bool), np.asarray(ref_tb, bool))
+        assert np.array_equal(cb_ok.numpy().astype(bool), np.asarray(ref_cb, bool))
+        assert np.array_equal(it.numpy().astype(np.uint32), np.asarray(ref_it, np.uint32))

@@ -649,6 +649,31 @@ class Decoder:
         _call("tc_derate_combine_llr_device", self._h, len(transmissions), C.addressof(arr),
               int(e_len), e_ptr, int(llr_len), out_ptr, stream or None)
 
+    @staticmethod
+    def tb_descriptors(tbs):
+        """tc_transport_block array for tbs = list of (TBS, n_cb) in order, bits back to back.
+        Returns (array, total decoded bits)."""
+        tba = (_TransportBlock * max(len(tbs), 1))()
+        first = bits = 0
+        for i, (size, ncb) in enumerate(tbs):
+            tba[i].tbs, tba[i].first_cb, tba[i].n_cb, tba[i].bits_offset = (
+                int(size), first, int(ncb), bits)
+            first += int(ncb)
+            bits += int(size)
+        return tba, bits
+
+    def decode_tbs_async(self, tba, n_tb: int, arr, n_cb: int, e_len: int, e_llr_ptr: int,
+                         bits_len: int, bits_ptr: int, tb_ok_ptr: int = 0, cb_ok_ptr: int = 0,
+                         iters_ptr: int = 0, options: Optional[DecodeOptions] = None) -> None:
+        """tc_decode_transport_blocks with TC_MEM_HOST_ASYNC: host pointers (pinned for
+        overlap), descriptors from tb_descriptors() and rm_blocks(); returns once enqueued.
+        Results are valid after sync()."""
+        o = options or DecodeOptions()
+        opt, _keep = self._opts(o, MEM_HOST_ASYNC)
+        _call("tc_decode_transport_blocks", self._h, int(n_tb), C.addressof(tba), int(n_cb),
+              C.addressof(arr), int(e_len), e_llr_ptr, int(bits_len), bits_ptr,
+              tb_ok_ptr or None, cb_ok_ptr or None, iters_ptr or None, None, C.addressof(opt))
+
     def decode_tbs(self, tbs, blocks, e_llr, options: Optional[DecodeOptions] = None,
                    want_posterior: bool = False):
         """Many transport blocks through the device chain (host arrays): tbs = list of
@@ -660,13 +685,7 @@ class Decoder:
         x = np.ascontiguousarray(e_llr, np.float32)
         if x.size != e_len:
             raise InvalidArgument(f"expected {e_len} rate-matched LLRs, got {x.size}")
-        tba = (_TransportBlock * max(len(tbs), 1))()
-        first = bits = 0
-        for i, (size, ncb) in enumerate(tbs):
-            tba[i].tbs, tba[i].first_cb, tba[i].n_cb, tba[i].bits_offset = (
-                int(size), first, int(ncb), bits)
-            first += int(ncb)
-            bits += int(size)
+        tba, bits = self.tb_descriptors(tbs)
         out = np.zeros(bits, np.uint8)
         tb_ok = np.zeros(len(tbs), np.uint8)
         cb_ok = np.zeros(len(blocks), np.uint8)

@@ -489,7 +489,10 @@ int tc_decode_transport_blocks(tc_decoder* dec, size_t n_tb, const tc_transport_
     q.cb_crc_ok = cb_crc_ok;
     q.iterations_used = iterations_used;
     q.posterior = posterior;
+    need(o.memory == TC_MEM_HOST || o.memory == TC_MEM_DEVICE || o.memory == TC_MEM_HOST_ASYNC,
+         "unknown memory kind");
     q.device_memory = o.memory == TC_MEM_DEVICE;
+    q.host_async = o.memory == TC_MEM_HOST_ASYNC;
     q.stream = o.stream;
     q.decode.max_iterations = o.max_iterations;
     q.decode.early_stop = o.early_stop != 0;

@@ -237,7 +237,29 @@ void Decoder::derate_match_llr(size_t n, const RmBlockDesc* blocks, const float*
   mark_done(stream);
 }
 
+// TC_MEM_HOST_ASYNC: the whole call goes to one of the worker decoders (own device buffers
+// and stream, used in turn) and is not waited for, so that one call's copies overlap earlier
+// calls' decoding; sync() waits for the workers.  Descriptor uploads read host vectors of this
+// call, which cudaMemcpyAsync stages before it returns.
 void Decoder::decode_transport_blocks(const TbRequest& q) {
+  if (q.host_async && !q.device_memory) {
+    std::lock_guard<std::mutex> lock(mu_);
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    while (workers_.size() < kAsyncWorkers) workers_.push_back(std::make_unique<Decoder>(device_));
+    Decoder& w = *workers_[next_worker_];
+    next_worker_ = (next_worker_ + 1) % workers_.size();
+    TbRequest r = q;
+    r.host_async = false;
+    r.stream = nullptr;  // the worker's own stream
+    const uint64_t launches_before = w.timing_.launches;
+    w.transport_blocks(r, false);
+    timing_.launches += w.timing_.launches - launches_before;
+    return;
+  }
+  transport_blocks(q, true);
+}
+
+void Decoder::transport_blocks(const TbRequest& q, bool wait) {
   std::lock_guard<std::mutex> lock(mu_);
   check(cudaSetDevice(device_), "cudaSetDevice");
   cudaStream_t st = static_cast<cudaStream_t>(q.device_memory ? q.stream
@@ -338,7 +360,7 @@ void Decoder::decode_transport_blocks(const TbRequest& q) {
                           cudaMemcpyDeviceToDevice, st), "copy");
   }
   mark_done(st);
-  if (!q.device_memory) {
+  if (!q.device_memory && wait) {
     check(cudaStreamSynchronize(st), "sync");
     if (rq.persistent) take_error();
   }

@@ -683,10 +683,6 @@ void Decoder::decode_plain(const DecodeRequest& rq) {
 // ------------------------------------------------------------------------------------------
 // Asynchronous host-memory calls
 // ------------------------------------------------------------------------------------------
-namespace {
-constexpr size_t kAsyncWorkers = 3;  // copy-in of call i+2 needs no wait for call i
-}  // namespace
-
 void Decoder::decode_host_async(const DecodeRequest& rq) {
   if (rq.n_cb == 0) return;
   check(cudaSetDevice(device_), "cudaSetDevice");

@@ -37,6 +37,7 @@ constexpr int kGroup = 8;            // load granularity: windows and guards are
 constexpr int kDefaultWindow = 128;  // window length (steps)
 constexpr int kDefaultGuard = 96;    // warm-up steps on each side of a window
 constexpr int kPersistWindow = 192;  // target window of the persistent schedule (<= 32 per block)
+constexpr size_t kAsyncWorkers = 3;  // TC_MEM_HOST_ASYNC workspaces: call i+2's copy-in needs no wait for call i
 
 struct CodeBlockDesc {
   int32_t k;
@@ -103,6 +104,7 @@ struct TbRequest {
   uint32_t* iterations_used = nullptr;  // n_cb
   float* posterior = nullptr;         // optional: sum K, blocks back to back
   bool device_memory = false;
+  bool host_async = false;            // host pointers; enqueued on a worker, valid after sync()
   void* stream = nullptr;
   DecodeRequest decode;               // iterations, early stop, schedule, window, guard, scales
 };
@@ -180,6 +182,7 @@ class Decoder {
   // Asynchronous host-memory calls rotate over kAsyncWorkers worker decoders, each with its own
   // device buffers and stream: a call enqueues copy-in, decode and copy-out on the next worker
   // and returns, so that its copies run while the previous calls decode.  sync() waits for them.
+  void transport_blocks(const TbRequest& q, bool wait);  // wait: synchronise host-memory calls
   void decode_host_async(const DecodeRequest& rq);
   std::vector<std::unique_ptr<Decoder>> workers_;
   size_t next_worker_ = 0;
