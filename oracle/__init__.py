@@ -91,6 +91,8 @@ class Oracle(_Lib):
         _sig(L, "or_adj_seed_count", C.c_int64, [C.c_int32, C.c_int32, C.c_int32])
         _sig(L, "or_adj_vjp", None,
              [C.c_int32, _f64p, C.c_int32, _f64p, C.c_int32, C.c_int32] + [_f64n] * 6)
+        _sig(L, "or_std_adj_vjp", None,
+             [C.c_int32, _f64p, C.c_int32, _f64p, C.c_int32, C.c_int32] + [_f64n] * 6)
 
     # -- QPP --
     def qpp_table(self):
@@ -201,10 +203,11 @@ class Oracle(_Lib):
         return post, bool(ok.value), used.value
 
     # -- FP64 differentiable decoder (scaled extrinsics, windowed schedule) and its adjoint --
-    def adj_vjp(self, k, llr, scales, window=0, guard=0, grad_post=None, frozen_seeds=None):
+    def adj_vjp(self, k, llr, scales, window=0, guard=0, grad_post=None, frozen_seeds=None,
+                std=False):
         """Returns (posterior, seeds used, grad_llr, grad_scales); the gradients are the
         vector-Jacobian product with grad_post (None: forward only, gradients None).
-        len(scales) // 2 iterations."""
+        len(scales) // 2 iterations.  std: the TS 36.212 code."""
         def ptr(a):
             return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
         scales = np.ascontiguousarray(scales, np.float64)
@@ -216,8 +219,9 @@ class Oracle(_Lib):
         gp = None if grad_post is None else np.ascontiguousarray(grad_post, np.float64)
         g_llr = np.empty(3 * (k + 4), np.float64) if gp is not None else None
         g_s = np.empty(scales.size, np.float64) if gp is not None else None
-        self.lib.or_adj_vjp(k, llr, iters, scales, window, guard, ptr(fz), ptr(gp), ptr(post),
-                            ptr(g_llr), ptr(g_s), ptr(seeds))
+        f = self.lib.or_std_adj_vjp if std else self.lib.or_adj_vjp
+        f(k, llr, iters, scales, window, guard, ptr(fz), ptr(gp), ptr(post), ptr(g_llr), ptr(g_s),
+          ptr(seeds))
         return post, seeds, g_llr, g_s
 
     def decode_batch(self, ks, fillers, llr, llr_off, out_off, iters=8, early_stop=False,

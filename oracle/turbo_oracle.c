@@ -840,17 +840,15 @@ static inline double gam(const trellis_t* T, int s, int u, double a, double b) {
 
 /* beta at the block end from the three termination steps (lte_turbo.cpp:357-378), and its
  * derivatives w.r.t. the tail systematic (ts) and parity (tp) LLRs */
-static void tail_beta64(const double ts[3], const double tp[3], double beta[8], double dts[8][3],
-                        double dtp[8][3]) {
+static void tail_beta64(const trellis_t* T, const double ts[3], const double tp[3], double beta[8],
+                        double dts[8][3], double dtp[8][3]) {
   for (int s = 0; s < 8; ++s) {
-    uint8_t cur = (uint8_t)s, in[3];
-    termination(cur, in);
+    uint8_t cur = (uint8_t)s;
     double m = 0.0;
     for (int i = 0; i < 3; ++i) {
-      uint8_t p, n;
-      rsc_step(cur, in[i], &p, &n);
-      cur = n;
-      dts[s][i] = in[i] ? 0.5 : -0.5;
+      const uint8_t in = T->term[cur], p = T->parity[cur][in];
+      cur = T->next[cur][in];
+      dts[s][i] = in ? 0.5 : -0.5;
       dtp[s][i] = p ? 0.5 : -0.5;
       m += dts[s][i] * ts[i] + dtp[s][i] * tp[i];
     }
@@ -901,7 +899,7 @@ static void seg64_forward(const trellis_t* T, const double* sys, const double* p
     for (int s = 0; s < 8; ++s) bk[s] = b_in[s];
   } else {
     double dts[8][3], dtp[8][3];
-    tail_beta64(ts, tp, bk, dts, dtp);
+    tail_beta64(T, ts, tp, bk, dts, dtp);
   }
   for (int32_t p = g.b_hi; p-- > g.lo;) {
     const double a = 0.5 * (sys[p] + apr[p]), b = 0.5 * par[p];
@@ -995,7 +993,7 @@ static void seg64_adjoint(const trellis_t* T, const double* sys, const double* p
   }
   if (g.tail) {
     double bk[8], dts[8][3], dtp[8][3];
-    tail_beta64(ts, tp, bk, dts, dtp);
+    tail_beta64(T, ts, tp, bk, dts, dtp);
     for (int s = 0; s < 8; ++s)
       for (int i = 0; i < 3; ++i) {
         g_ts[i] += bb[8 * (nb - 1) + s] * dts[s][i];
@@ -1018,10 +1016,15 @@ int64_t or_adj_seed_count(int32_t k, int32_t iters, int32_t window) {
 /* tail LLRs of both SISOs (gather_tails, lte_turbo.cpp:758-773) and where they come from in
  * [d0|d1|d2] (offsets into the 3(K+4) LLRs) */
 static void tails64(int32_t k, const double* llr, double ts[2][3], double tp[2][3],
-                    int32_t its[2][3], int32_t itp[2][3]) {
+                    int32_t its[2][3], int32_t itp[2][3], int std) {
   const int32_t o0 = 0, o1 = k + 4, o2 = 2 * (k + 4);
-  const int32_t s_idx[2][3] = {{o0 + k, o0 + k + 2, -1}, {o1 + k + 3, o2 + k, o2 + k + 2}};
-  const int32_t p_idx[2][3] = {{o1 + k, o0 + k + 1, o1 + k + 2}, {o2 + k + 1, o0 + k + 3, o2 + k + 3}};
+  const int32_t r_s[2][3] = {{o0 + k, o0 + k + 2, -1}, {o1 + k + 3, o2 + k, o2 + k + 2}};
+  const int32_t r_p[2][3] = {{o1 + k, o0 + k + 1, o1 + k + 2}, {o2 + k + 1, o0 + k + 3, o2 + k + 3}};
+  /* TS 36.212 5.1.3.2.2 (gather_tails_std) */
+  const int32_t t_s[2][3] = {{o0 + k, o2 + k, o1 + k + 1}, {o0 + k + 2, o2 + k + 2, o1 + k + 3}};
+  const int32_t t_p[2][3] = {{o1 + k, o0 + k + 1, o2 + k + 1}, {o1 + k + 2, o0 + k + 3, o2 + k + 3}};
+  const int32_t(*s_idx)[3] = std ? t_s : r_s;
+  const int32_t(*p_idx)[3] = std ? t_p : r_p;
   for (int h = 0; h < 2; ++h)
     for (int i = 0; i < 3; ++i) {
       its[h][i] = s_idx[h][i];
@@ -1031,11 +1034,11 @@ static void tails64(int32_t k, const double* llr, double ts[2][3], double tp[2][
     }
 }
 
-void or_adj_vjp(int32_t k, const double* llr, int32_t iters, const double* scales,
-                int32_t window, int32_t guard, const double* frozen_seeds,
-                const double* grad_post, double* posterior, double* grad_llr,
-                double* grad_scales, double* seeds_out) {
-  const trellis_t T = make_trellis();
+static void adj_vjp(int32_t k, const double* llr, int32_t iters, const double* scales,
+                    int32_t window, int32_t guard, const double* frozen_seeds,
+                    const double* grad_post, double* posterior, double* grad_llr,
+                    double* grad_scales, double* seeds_out, int std) {
+  const trellis_t T = make_trellis_conv(std);
   const int32_t W = adj_window(k, window);
   const int32_t G = guard < 0 ? 0 : (guard > W ? W : guard);
   const int32_t nw = (k + W - 1) / W, nj = 2 * iters;
@@ -1044,7 +1047,7 @@ void or_adj_vjp(int32_t k, const double* llr, int32_t iters, const double* scale
   const double* d2 = llr + 2 * (k + 4);
   double ts[2][3], tp[2][3];
   int32_t its[2][3], itp[2][3];
-  tails64(k, llr, ts, tp, its, itp);
+  tails64(k, llr, ts, tp, its, itp, std);
   int32_t* perm = (int32_t*)malloc(sizeof(int32_t) * (size_t)k);
   or_qpp_perm(k, perm);
   const size_t rows = (size_t)(W + 2 * G + 1);
@@ -1162,4 +1165,21 @@ void or_adj_vjp(int32_t k, const double* llr, int32_t iters, const double* scale
   }
   free(perm); free(alpha); free(beta); free(sys_i); free(e1); free(e2); free(x);
   free(tape_apr); free(tape_x); free(seeds);
+}
+
+void or_adj_vjp(int32_t k, const double* llr, int32_t iters, const double* scales,
+                int32_t window, int32_t guard, const double* frozen_seeds,
+                const double* grad_post, double* posterior, double* grad_llr,
+                double* grad_scales, double* seeds_out) {
+  adj_vjp(k, llr, iters, scales, window, guard, frozen_seeds, grad_post, posterior, grad_llr,
+          grad_scales, seeds_out, 0);
+}
+
+/* The same on the TS 36.212 code (trellis, termination, tail mapping). */
+void or_std_adj_vjp(int32_t k, const double* llr, int32_t iters, const double* scales,
+                    int32_t window, int32_t guard, const double* frozen_seeds,
+                    const double* grad_post, double* posterior, double* grad_llr,
+                    double* grad_scales, double* seeds_out) {
+  adj_vjp(k, llr, iters, scales, window, guard, frozen_seeds, grad_post, posterior, grad_llr,
+          grad_scales, seeds_out, 1);
 }

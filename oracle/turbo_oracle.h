@@ -119,6 +119,12 @@ void or_std_decode_cb_windowed(int32_t k, int32_t filler, const float* llr,
                                int32_t guard, float* posterior, int32_t* crc_ok,
                                int32_t* iterations_used);
 
+/* The FP64 differentiable decoder and its adjoint (or_adj_vjp) on the TS 36.212 code. */
+void or_std_adj_vjp(int32_t k, const double* llr, int32_t iters, const double* scales,
+                    int32_t window, int32_t guard, const double* frozen_seeds,
+                    const double* grad_post, double* posterior, double* grad_llr,
+                    double* grad_scales, double* seeds_out);
+
 #ifdef __cplusplus
 }
 #endif
