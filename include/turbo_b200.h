@@ -160,7 +160,8 @@ typedef struct {
                               early stop; CRC24A too in tc_decode_transport_blocks).  Honoured
                               by tc_decode (every schedule and memory kind), tc_autotune and
                               tc_decode_transport_blocks; tc_decode_noalloc refuses the 3GPP
-                              code (TC_ERR_INVALID_ARGUMENT); the adjoint is the reference's */
+                              code (TC_ERR_INVALID_ARGUMENT); the differentiable decoder takes
+                              it through tc_adjoint_forward_conv */
 } tc_decode_options;
 
 TC_API int tc_decode_options_init(tc_decode_options* opts);
@@ -324,6 +325,13 @@ TC_API int tc_adjoint_forward(tc_adjoint* adj, size_t n_cb, const tc_code_block*
                               size_t llr_len, const float* llr, size_t post_len, float* posterior,
                               uint32_t iterations, const float* scales, int32_t window,
                               int32_t guard, void* stream, uint64_t* tape);
+/* The same on the code `convention` selects (TC_CONVENTION_REFERENCE or TC_CONVENTION_3GPP);
+ * the backward pass differentiates the code of its tape. */
+TC_API int tc_adjoint_forward_conv(int convention, tc_adjoint* adj, size_t n_cb,
+                                   const tc_code_block* cbs, size_t llr_len, const float* llr,
+                                   size_t post_len, float* posterior, uint32_t iterations,
+                                   const float* scales, int32_t window, int32_t guard,
+                                   void* stream, uint64_t* tape);
 /* grad_posterior: post_len floats (posterior layout); grad_llr: llr_len floats (LLR layout,
  * 0 outside every block); grad_scales: 2*iterations floats. */
 TC_API int tc_adjoint_backward(tc_adjoint* adj, uint64_t tape, const float* grad_posterior,

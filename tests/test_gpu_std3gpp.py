@@ -220,3 +220,107 @@ def test_std_async_host_calls_and_autotuned_schedule(tc):
                       stream=s.cuda_stream)
     s.synchronize()
     assert np.array_equal((out.cpu().numpy() >= 0).astype(np.uint8), np.concatenate(cb_bits))
+
+
+# ---- the differentiable decoder on the 36.212 code (bars as tests/test_gpu_adjoint.py) ----
+H_FD = 1e-4
+RTOL_ADJ = 1e-4
+
+
+def _std_gpu_vjp(tc, decoder, ks, llr, bits, scales, window=0, guard=-1):
+    """GPU forward + backward on the 36.212 code: (posterior, d loss/d posterior, grad_llr,
+    grad_scales), loss = mean BCE against the code-block bits."""
+    import torch
+
+    adj = tc.AdjointDecoder(decoder)
+    iters = len(scales) // 2
+    cbs, llr_len, post_len = tc.Decoder.layout(ks)
+    s = torch.cuda.current_stream().cuda_stream
+    x = torch.from_numpy(np.ascontiguousarray(llr, np.float32)).cuda()
+    post = torch.zeros(post_len, device="cuda")
+    tape = adj.forward(cbs, len(ks), x.data_ptr(), llr_len, post.data_ptr(), post_len, iters,
+                       scales, window, guard, stream=s, convention=tc.CONVENTION_3GPP)
+    b = torch.from_numpy(np.concatenate(bits).astype(np.float32)).cuda()
+    gp = (torch.sigmoid(post) - b) / post.numel()
+    gl = torch.zeros(llr_len, device="cuda")
+    gs = torch.zeros(2 * iters, device="cuda")
+    adj.backward(tape, gp.data_ptr(), gl.data_ptr(), gs.data_ptr(), stream=s)
+    torch.cuda.synchronize()
+    return post.cpu().numpy(), gp.cpu().numpy(), gl.cpu().numpy(), gs.cpu().numpy()
+
+
+def _rel(got, ref):
+    return float(np.abs(got - ref).max() / np.abs(ref).max())
+
+
+def test_std_adjoint_gradient_check_k40(tc, decoder, oracle):
+    """8 blocks of K=40 at 0.6 dB, 6 iterations, 12 scales: GPU gradients on the 36.212 code vs
+    FP64 central differences of the oracle's 36.212 loss and vs its FP64 adjoint."""
+    n, k, iters = 8, 40, 6
+    llr, bits = std_code_blocks(tc, [k] * n, 0.6, seed=50)
+    scales = np.random.default_rng(2).uniform(0.6, 1.2, 2 * iters)
+    post, gp, g_llr, g_s = _std_gpu_vjp(tc, decoder, [k] * n, llr, bits,
+                                        scales.astype(np.float32))
+    l64 = llr.astype(np.float64).reshape(n, 3 * (k + 4))
+    b64 = [b.astype(np.float64) for b in bits]
+
+    def block_loss(i, l, s):
+        p = oracle.adj_vjp(k, l, s, std=True)[0]
+        return float(np.sum(np.logaddexp(0.0, p) - b64[i] * p)) / (n * k)
+
+    fd_s = np.array([sum(block_loss(i, l64[i], scales + H_FD * e)
+                         - block_loss(i, l64[i], scales - H_FD * e) for i in range(n)) / (2 * H_FD)
+                     for e in np.eye(2 * iters)])
+    fd_l = np.array([[(block_loss(i, l64[i] + H_FD * e, scales)
+                       - block_loss(i, l64[i] - H_FD * e, scales)) / (2 * H_FD)
+                      for e in np.eye(l64.shape[1])] for i in range(n)]).ravel()
+    a_l, a_s = [], np.zeros(2 * iters)
+    for i in range(n):
+        p = oracle.adj_vjp(k, l64[i], scales, std=True)[0]
+        _, _, g, s_ = oracle.adj_vjp(k, l64[i], scales,
+                                     grad_post=(1 / (1 + np.exp(-p)) - b64[i]) / (n * k), std=True)
+        a_l.append(g)
+        a_s += s_
+    a_l = np.concatenate(a_l)
+    err = dict(fp64_scales_fd=_rel(a_s, fd_s), fp64_llr_fd=_rel(a_l, fd_l),
+               scales_fd=_rel(g_s, fd_s), llr_fd=_rel(g_llr, fd_l), scales_adj=_rel(g_s, a_s),
+               llr_adj=_rel(g_llr, a_l))
+    print("36.212 K=40 gradient check (max rel):", err)
+    assert err["fp64_scales_fd"] < 1e-5 and err["fp64_llr_fd"] < 1e-5, err
+    assert max(err[key] for key in ("scales_fd", "llr_fd", "scales_adj", "llr_adj")) < RTOL_ADJ, err
+
+
+def test_std_adjoint_windowed_vjp_and_autograd(tc, decoder, oracle):
+    """K=1024, window 64, guard 32, 6 iterations on the 36.212 code: the GPU posterior and
+    vector-Jacobian product against the FP64 36.212 adjoint fed the same d loss / d posterior;
+    the torch autograd wrapper gives the same gradients."""
+    import torch
+    from turbo_cpp_b200.autograd import DifferentiableDecoder
+
+    k, n, iters = 1024, 4, 6
+    llr, bits = std_code_blocks(tc, [k] * n, 0.6, seed=51)
+    scales = np.random.default_rng(5).uniform(0.7, 1.1, 2 * iters).astype(np.float32)
+    post, gp, g_llr, g_s = _std_gpu_vjp(tc, decoder, [k] * n, llr, bits, scales, 64, 32)
+    p64, a_l, a_s = [], [], np.zeros(2 * iters)
+    for i in range(n):
+        seg = llr[i * 3 * (k + 4):(i + 1) * 3 * (k + 4)].astype(np.float64)
+        p, _, g, s_ = oracle.adj_vjp(k, seg, scales.astype(np.float64), 64, 32,
+                                     grad_post=gp[i * k:(i + 1) * k].astype(np.float64), std=True)
+        p64.append(p)
+        a_l.append(g)
+        a_s += s_
+    err = dict(post=_rel(post, np.concatenate(p64)), scales=_rel(g_s, a_s),
+               llr=_rel(g_llr, np.concatenate(a_l)))
+    print("36.212 K=1024 windowed (max rel):", err)
+    assert err["post"] < 1e-4 and err["scales"] < RTOL_ADJ and err["llr"] < RTOL_ADJ, err
+
+    dd = DifferentiableDecoder([k] * n, window=64, guard=32, decoder=decoder,
+                               convention=tc.CONVENTION_3GPP)
+    x = torch.from_numpy(np.ascontiguousarray(llr, np.float32)).cuda().requires_grad_(True)
+    sc = torch.from_numpy(scales).cuda().requires_grad_(True)
+    out = dd(x, sc)
+    b = torch.from_numpy(np.concatenate(bits).astype(np.float32)).cuda()
+    torch.nn.functional.binary_cross_entropy_with_logits(out, b).backward()
+    assert np.array_equal(out.detach().cpu().numpy(), post)
+    assert np.allclose(x.grad.cpu().numpy(), g_llr, rtol=0, atol=1e-5 * np.abs(g_llr).max())
+    assert np.allclose(sc.grad.cpu().numpy(), g_s, rtol=1e-4, atol=0)

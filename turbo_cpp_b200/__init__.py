@@ -161,6 +161,8 @@ _SIGNATURES = {
     "tc_adjoint_destroy": [_VP],
     "tc_adjoint_forward": [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, C.c_uint32, _VP, C.c_int32,
                            C.c_int32, _VP, _VP],
+    "tc_adjoint_forward_conv": [C.c_int, _VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, C.c_uint32, _VP,
+                                C.c_int32, C.c_int32, _VP, _VP],
     "tc_adjoint_backward": [_VP, C.c_uint64, _VP, _VP, _VP, _VP],
     "tc_adjoint_launches": [_VP, _VP],
 }
@@ -784,17 +786,19 @@ class AdjointDecoder:
 
     def forward(self, cbs, n_cb: int, llr_ptr: int, llr_len: int, post_ptr: int, post_len: int,
                 iterations: int, scales=None, window: int = 0, guard: int = -1,
-                stream: int = 0) -> int:
-        """Decodes and records the tape; returns the tape id for backward()."""
+                stream: int = 0, convention: int = CONVENTION_REFERENCE) -> int:
+        """Decodes and records the tape; returns the tape id for backward().  convention: the
+        code of the LLRs (CONVENTION_REFERENCE or CONVENTION_3GPP)."""
         sc = None
         if scales is not None:
             sc = np.ascontiguousarray(scales, np.float32)
             if sc.size != 2 * iterations:
                 raise InvalidArgument("scales: two per iteration")
         tape = C.c_uint64()
-        _call("tc_adjoint_forward", self._h, int(n_cb), C.addressof(cbs), int(llr_len), llr_ptr,
-              int(post_len), post_ptr, int(iterations), None if sc is None else _ptr(sc),
-              int(window), int(guard), stream or None, C.addressof(tape))
+        _call("tc_adjoint_forward_conv", int(convention), self._h, int(n_cb), C.addressof(cbs),
+              int(llr_len), llr_ptr, int(post_len), post_ptr, int(iterations),
+              None if sc is None else _ptr(sc), int(window), int(guard), stream or None,
+              C.addressof(tape))
         return tape.value
 
     def backward(self, tape: int, grad_post_ptr: int, grad_llr_ptr: int, grad_scales_ptr: int,

@@ -31,11 +31,12 @@ def extension():
 class DifferentiableDecoder:
     """posterior = dd(llr, scales) for blocks of sizes ``ks`` stored back to back
     ([d0|d1|d2] per block, K posteriors per block), ``len(scales) // 2`` unrolled iterations
-    without early stop, on the windowed schedule (window, guard; 0 / -1 = 64 / 32)."""
+    without early stop, on the windowed schedule (window, guard; 0 / -1 = 64 / 32), for the
+    code ``convention`` names (CONVENTION_REFERENCE or CONVENTION_3GPP)."""
 
     def __init__(self, ks: Sequence[int], fillers: Optional[Sequence[int]] = None,
                  window: int = 0, guard: int = -1, device: int = 0,
-                 decoder: Optional[Decoder] = None):
+                 decoder: Optional[Decoder] = None, convention: int = 0):
         import torch
 
         self.decoder = decoder or Decoder(device)
@@ -45,10 +46,11 @@ class DifferentiableDecoder:
             [[cbs[i].k, cbs[i].filler, cbs[i].llr_offset, cbs[i].out_offset] for i in range(len(ks))],
             dtype=torch.int64)
         self.window, self.guard = int(window), int(guard)
+        self.convention = int(convention)
         self._ext = extension()
 
     def __call__(self, llr, scales):
         if llr.numel() != self.llr_len:
             raise ValueError("llr: wrong length for these blocks")
         return self._ext.decode(llr, scales, self.adjoint._h.value, self.code_blocks,
-                                self.post_len, self.window, self.guard)
+                                self.post_len, self.window, self.guard, self.convention)

@@ -61,42 +61,46 @@ __device__ __forceinline__ void pair_weights(float x0, float x1, float& w0, floa
 }
 
 // d(alpha_{p+1}) -> d(alpha_p): ab += J^T abn, with J the softmax weights of alpha_step at p;
-// ga, gb accumulate d/da and d/db of the step's branch metrics.
+// ga, gb accumulate d/da and d/db of the step's branch metrics.  (In the reference's trellis
+// both predecessors of a state enter it with the same input; in the TS 36.212 one (STD) they
+// differ.)
+template <bool STD = false>
 __device__ __forceinline__ void alpha_adjoint(const float (&al)[8], float a, float b,
                                               const float (&abn)[8], float (&ab)[8], float& ga,
                                               float& gb) {
   const float g0 = a + b, g1 = a - b;
 #pragma unroll
   for (int n = 0; n < 8; ++n) {
-    const int n2 = (n >> 2) & 1, n1 = (n >> 1) & 1, n0 = n & 1;
-    const int u = n2 ^ n1 ^ n0;
     const int p0 = 2 * (n & 3);
-    const int par0 = n2 ^ n1, par1 = n2 ^ n1 ^ 1;
+    const int u0 = pred_input<STD>(n, 0), u1 = pred_input<STD>(n, 1);
+    const int par0 = pred_parity(n, 0), par1 = pred_parity(n, 1);
     float w0, w1;
-    pair_weights(al[p0] + branch(u, par0, g0, g1), al[p0 + 1] + branch(u, par1, g0, g1), w0, w1);
+    pair_weights(al[p0] + branch(u0, par0, g0, g1), al[p0 + 1] + branch(u1, par1, g0, g1), w0,
+                 w1);
     const float q0 = w0 * abn[n], q1 = w1 * abn[n];
     ab[p0] += q0;
     ab[p0 + 1] += q1;
-    ga += u ? (q0 + q1) : -(q0 + q1);
+    ga += u0 == u1 ? (u0 ? (q0 + q1) : -(q0 + q1)) : (u0 ? q0 : -q0) + (u1 ? q1 : -q1);
     gb += (par0 ? q0 : -q0) + (par1 ? q1 : -q1);
   }
 }
 
 // d(beta_p) -> d(beta_{p+1}): bbn += J^T bb, J the softmax weights of beta_step at p (bn holds
 // beta_{p+1}).
+template <bool STD = false>
 __device__ __forceinline__ void beta_adjoint(const float (&bn)[8], float a, float b,
                                              const float (&bb)[8], float (&bbn)[8], float& ga,
                                              float& gb) {
   const float g0 = a + b, g1 = a - b;
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
-    const int pa0 = parity(s, 0), pa1 = parity(s, 1);
+    const int pa0 = parity<STD>(s, 0), pa1 = parity<STD>(s, 1);
     float w0, w1;
-    pair_weights(bn[next_state(s, 0)] + branch(0, pa0, g0, g1),
-                 bn[next_state(s, 1)] + branch(1, pa1, g0, g1), w0, w1);
+    pair_weights(bn[next_state<STD>(s, 0)] + branch(0, pa0, g0, g1),
+                 bn[next_state<STD>(s, 1)] + branch(1, pa1, g0, g1), w0, w1);
     const float q0 = w0 * bb[s], q1 = w1 * bb[s];
-    bbn[next_state(s, 0)] += q0;
-    bbn[next_state(s, 1)] += q1;
+    bbn[next_state<STD>(s, 0)] += q0;
+    bbn[next_state<STD>(s, 1)] += q1;
     ga += q1 - q0;
     gb += (pa0 ? q0 : -q0) + (pa1 ? q1 : -q1);
   }
@@ -104,14 +108,14 @@ __device__ __forceinline__ void beta_adjoint(const float (&bn)[8], float a, floa
 
 // Softmax weights of the two 8-way log-sums of the extrinsic (extrinsic2): w_u[s] is the weight
 // of branch (s, u) in the u-side log-sum.  Returns the base-2 extrinsic when WANT_VALUE.
-template <bool WANT_VALUE>
+template <bool WANT_VALUE, bool STD = false>
 __device__ __forceinline__ float ext_weights(const float (&al)[8], const float (&be)[8], float b,
                                              float (&w0)[8], float (&w1)[8]) {
   float m0[8], m1[8];
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
-    m0[s] = al[s] + be[next_state(s, 0)] + (parity(s, 0) ? b : -b);
-    m1[s] = al[s] + be[next_state(s, 1)] + (parity(s, 1) ? b : -b);
+    m0[s] = al[s] + be[next_state<STD>(s, 0)] + (parity<STD>(s, 0) ? b : -b);
+    m1[s] = al[s] + be[next_state<STD>(s, 1)] + (parity<STD>(s, 1) ? b : -b);
   }
   const float x0 = fmaxf(fmaxf(fmaxf(m0[0], m0[1]), fmaxf(m0[2], m0[3])),
                          fmaxf(fmaxf(m0[4], m0[5]), fmaxf(m0[6], m0[7])));
@@ -177,7 +181,7 @@ __device__ __forceinline__ void load_ge(const AdjIo& io, const DevCb& cb, bool l
 // spilled) fit where the single kernel held 4 (234 registers); measured 8.63 against 8.94 ms
 // for the 12 backward half-iterations of 1024 blocks of K=6144.
 constexpr int kAdjMinBlocks = 6;
-template <bool LOWER, int PHASES>
+template <bool LOWER, int PHASES, bool STD = false>
 __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kernel(const DevCb* __restrict__ cbs,
                                                                   const int32_t* __restrict__ win_cb,
                                                                   int n_win, AdjIo io) {
@@ -209,15 +213,15 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
     cka.store((q - a_lo) >> 2, al);
     scale4(load_raw4(sys, apr, par, q), sa, a, b);
 #pragma unroll
-    for (int t = 0; t < 4; ++t) alpha_step(al, a[t], b[t]);
+    for (int t = 0; t < 4; ++t) alpha_step<STD>(al, a[t], b[t]);
   }
 
   // ---- B: backward in time ----
   float be[8];
   if (tail) {
     float ts[3], tp[3];
-    tail_llrs(LOWER, d0, K, ts, tp);
-    tail_beta(be, ts, tp);
+    tail_llrs<STD>(LOWER, d0, K, ts, tp);
+    tail_beta<STD>(be, ts, tp);
   } else {
     load8(io.seeds + 16 * g + 8, be);
   }
@@ -225,7 +229,7 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
     ckb.store((P - lo) >> 2, be);
     scale4(load_raw4(sys, apr, par, P - 4), sa, a, b);
 #pragma unroll
-    for (int t = 3; t >= 0; --t) beta_step(be, a[t], b[t]);
+    for (int t = 3; t >= 0; --t) beta_step<STD>(be, a[t], b[t]);
   }
   float ab[8];
 #pragma unroll
@@ -243,25 +247,25 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
     for (int t = 0; t < 3; ++t) {
 #pragma unroll
       for (int s = 0; s < 8; ++s) Al[t + 1][s] = Al[t][s];
-      alpha_step(Al[t + 1], a[t], b[t]);
+      alpha_step<STD>(Al[t + 1], a[t], b[t]);
     }
     float gsa[4], gpar[4];
 #pragma unroll
     for (int t = 3; t >= 0; --t) {
       float w0[8], w1[8];
-      const float d2 = ext_weights<true>(Al[t], be, b[t], w0, w1);
+      const float d2 = ext_weights<true, STD>(Al[t], be, b[t], w0, w1);
       spart += ge[t] * (kLn2 * d2);
       const float G2 = xs * ge[t];
       float nab[8], ga = 0.0f, gb = 0.0f;
 #pragma unroll
       for (int s = 0; s < 8; ++s) {
         nab[s] = G2 * (w1[s] - w0[s]);
-        gb += G2 * ((parity(s, 1) ? w1[s] : -w1[s]) - (parity(s, 0) ? w0[s] : -w0[s]));
+        gb += G2 * ((parity<STD>(s, 1) ? w1[s] : -w1[s]) - (parity<STD>(s, 0) ? w0[s] : -w0[s]));
       }
-      alpha_adjoint(Al[t], a[t], b[t], ab, nab, ga, gb);
+      alpha_adjoint<STD>(Al[t], a[t], b[t], ab, nab, ga, gb);
 #pragma unroll
       for (int s = 0; s < 8; ++s) ab[s] = nab[s];
-      beta_step(be, a[t], b[t]);
+      beta_step<STD>(be, a[t], b[t]);
       gsa[t] = kHalfLog2e * ga;
       gpar[t] = kHalfLog2e * gb;
     }
@@ -277,7 +281,7 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
     for (int t = 0; t < 3; ++t) {
 #pragma unroll
       for (int s = 0; s < 8; ++s) Al[t + 1][s] = Al[t][s];
-      alpha_step(Al[t + 1], a[t], b[t]);
+      alpha_step<STD>(Al[t + 1], a[t], b[t]);
     }
     float gsa[4], gpar[4];
 #pragma unroll
@@ -285,7 +289,7 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
       float nab[8], ga = 0.0f, gb = 0.0f;
 #pragma unroll
       for (int s = 0; s < 8; ++s) nab[s] = 0.0f;
-      alpha_adjoint(Al[t], a[t], b[t], ab, nab, ga, gb);
+      alpha_adjoint<STD>(Al[t], a[t], b[t], ab, nab, ga, gb);
 #pragma unroll
       for (int s = 0; s < 8; ++s) ab[s] = nab[s];
       gsa[t] = kHalfLog2e * ga;
@@ -313,7 +317,7 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
     for (int t = 3; t > 0; --t) {
 #pragma unroll
       for (int s = 0; s < 8; ++s) Bt[t - 1][s] = Bt[t][s];
-      beta_step(Bt[t - 1], a[t], b[t]);
+      beta_step<STD>(Bt[t - 1], a[t], b[t]);
     }
     const bool own = P < hi;
     float ge[4] = {0.0f, 0.0f, 0.0f, 0.0f};
@@ -324,17 +328,17 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
       float nbb[8], ga = 0.0f, gb = 0.0f;
 #pragma unroll
       for (int s = 0; s < 8; ++s) nbb[s] = 0.0f;
-      beta_adjoint(Bt[t], a[t], b[t], bb, nbb, ga, gb);
+      beta_adjoint<STD>(Bt[t], a[t], b[t], bb, nbb, ga, gb);
       if (own) {
         float w0[8], w1[8];
-        ext_weights<false>(al, Bt[t], b[t], w0, w1);
+        ext_weights<false, STD>(al, Bt[t], b[t], w0, w1);
         const float G2 = xs * ge[t];
 #pragma unroll
         for (int s = 0; s < 8; ++s) {
-          nbb[next_state(s, 0)] -= G2 * w0[s];
-          nbb[next_state(s, 1)] += G2 * w1[s];
+          nbb[next_state<STD>(s, 0)] -= G2 * w0[s];
+          nbb[next_state<STD>(s, 1)] += G2 * w1[s];
         }
-        alpha_step(al, a[t], b[t]);
+        alpha_step<STD>(al, a[t], b[t]);
       }
 #pragma unroll
       for (int s = 0; s < 8; ++s) bb[s] = nbb[s];
@@ -360,11 +364,11 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
       int s = s0;
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
-        const int u = ((s >> 1) & 1) ^ ((s >> 2) & 1);
-        const int p = parity(s, u);
+        const int u = termination_input<STD>(s);
+        const int p = parity<STD>(s, u);
         gt[i] += u ? bb[s0] : -bb[s0];
         gt[3 + i] += p ? bb[s0] : -bb[s0];
-        s = next_state(s, u);
+        s = next_state<STD>(s, u);
       }
     }
     float* o = io.tail_g + 8 * g;
@@ -392,7 +396,7 @@ struct CombineIo {
 
 // One thread per position of the SISO's order: own + neighbours' warm-up gradients, then
 // d0/d1/d2 and the adjoint of the a-priori (the other SISO's scaled extrinsic).
-template <bool LOWER, bool LAST>
+template <bool LOWER, bool LAST, bool STD = false>
 __global__ void adj_combine_kernel(CombineIo c) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= c.total) return;
@@ -438,7 +442,15 @@ __global__ void adj_combine_kernel(CombineIo c) {
       const float* t = c.tail_g + 8 * (cb.win0 + v);
       for (int k = 0; k < 6; ++k) gt[k] += t[k];
     }
-    if (!LOWER) {  // ts = {d0[K], d0[K+2], 0}, tp = {d1[K], d0[K+1], d1[K+2]}
+    if (STD) {  // 36.212: ts = {d0[K+o], d2[K+o], d1[K+o+1]}, tp = {d1[K+o], d0[K+o+1], d2[K+o+1]}
+      const int o = LOWER ? 2 : 0;
+      g0[K + o] += gt[0];
+      g2[K + o] += gt[1];
+      g1[K + o + 1] += gt[2];
+      g1[K + o] += gt[3];
+      g0[K + o + 1] += gt[4];
+      g2[K + o + 1] += gt[5];
+    } else if (!LOWER) {  // ts = {d0[K], d0[K+2], 0}, tp = {d1[K], d0[K+1], d1[K+2]}
       g0[K] += gt[0];
       g0[K + 2] += gt[1];
       g1[K] += gt[3];
@@ -559,6 +571,7 @@ uint64_t Adjoint::forward(const AdjointRequest& rq) {
   guard_ = guard;
   iterations_ = I;
   llr_ = rq.llr;
+  std3gpp_ = rq.std3gpp;
   scales_.assign(2 * I, 1.0f);
   if (rq.scales) std::copy(rq.scales, rq.scales + 2 * I, scales_.begin());
   ckpt_fwd_ = max_window / kSub;
@@ -589,12 +602,21 @@ uint64_t Adjoint::forward(const AdjointRequest& rq) {
     SisoIo io{rq.llr, sysi, tape + j * work, tape + (j + 1) * work,
               (j + 1 == 2 * I) ? rq.posterior : nullptr, dperm, dinv, seeds + j * slab,
               seeds + (j + 2) * slab, scales_[j], guard};
-    if (!lower)
-      siso_plain_kernel<kSub, 0, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
-    else if (j + 1 < 2 * I)
-      siso_plain_kernel<kSub, 1, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
-    else
-      siso_plain_kernel<kSub, 2, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
+    if (rq.std3gpp) {
+      if (!lower)
+        siso_plain_kernel<kSub, 0, true, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
+      else if (j + 1 < 2 * I)
+        siso_plain_kernel<kSub, 1, true, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
+      else
+        siso_plain_kernel<kSub, 2, true, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
+    } else {
+      if (!lower)
+        siso_plain_kernel<kSub, 0, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
+      else if (j + 1 < 2 * I)
+        siso_plain_kernel<kSub, 1, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
+      else
+        siso_plain_kernel<kSub, 2, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
+    }
     ok(cudaGetLastError(), "SISO launch");
     launches_ += 1;
   }
@@ -641,7 +663,15 @@ void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr
     AdjIo io{llr_, sysi, tape + j * work, lower ? ge2 : ga1, dperm, seeds + j * slab, own,
              own + work, guard_g, tail_g, part + static_cast<int64_t>(j) * n_win, ckpt, ckpt_bwd_,
              scales_[j], G};
-    if (lower) {
+    if (std3gpp_) {
+      if (lower) {
+        siso_adjoint_kernel<true, 1, true><<<blocks, kAdjThreads, 0, st>>>(dcbs, dwin, n_win, io);
+        siso_adjoint_kernel<true, 2, true><<<blocks, kAdjThreads, 0, st>>>(dcbs, dwin, n_win, io);
+      } else {
+        siso_adjoint_kernel<false, 1, true><<<blocks, kAdjThreads, 0, st>>>(dcbs, dwin, n_win, io);
+        siso_adjoint_kernel<false, 2, true><<<blocks, kAdjThreads, 0, st>>>(dcbs, dwin, n_win, io);
+      }
+    } else if (lower) {
       siso_adjoint_kernel<true, 1><<<blocks, kAdjThreads, 0, st>>>(dcbs, dwin, n_win, io);
       siso_adjoint_kernel<true, 2><<<blocks, kAdjThreads, 0, st>>>(dcbs, dwin, n_win, io);
     } else {
@@ -651,12 +681,20 @@ void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr
     ok(cudaGetLastError(), "SISO adjoint launch");
     CombineIo c{dcbs, dstart, n, work, G, own, own + work, guard_g, tail_g, dperm, grad_post,
                 grad_llr, lower ? ga1 : ge2};
-    if (lower && last)
+    if (std3gpp_) {
+      if (lower && last)
+        adj_combine_kernel<true, true, true><<<pos_blocks, 256, 0, st>>>(c);
+      else if (lower)
+        adj_combine_kernel<true, false, true><<<pos_blocks, 256, 0, st>>>(c);
+      else
+        adj_combine_kernel<false, false, true><<<pos_blocks, 256, 0, st>>>(c);
+    } else if (lower && last) {
       adj_combine_kernel<true, true><<<pos_blocks, 256, 0, st>>>(c);
-    else if (lower)
+    } else if (lower) {
       adj_combine_kernel<true, false><<<pos_blocks, 256, 0, st>>>(c);
-    else
+    } else {
       adj_combine_kernel<false, false><<<pos_blocks, 256, 0, st>>>(c);
+    }
     ok(cudaGetLastError(), "adjoint combine launch");
     launches_ += 3;
   }

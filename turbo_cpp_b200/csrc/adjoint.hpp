@@ -33,6 +33,7 @@ struct AdjointRequest {
   int window = 0;                      // 0: kAdjWindow
   int guard = -1;                      // <0: kAdjGuard
   void* stream = nullptr;              // cudaStream_t (NULL = legacy default stream)
+  bool std3gpp = false;                // the TS 36.212 code instead of the reference's
 };
 
 class Adjoint {
@@ -63,6 +64,7 @@ class Adjoint {
   int64_t work_ = 0;
   int n_win_ = 0, guard_ = 0, ckpt_fwd_ = 0, ckpt_bwd_ = 0;
   uint32_t iterations_ = 0;
+  bool std3gpp_ = false;
   std::vector<float> scales_;
   const float* llr_ = nullptr;
   DeviceBuffer d_cbs_, d_wincb_, d_start_, d_sysi_, d_tape_, d_seeds_, d_ckpt_;

@@ -539,6 +539,15 @@ int tc_adjoint_forward(tc_adjoint* adj, size_t n_cb, const tc_code_block* cbs, s
                        const float* llr, size_t post_len, float* posterior, uint32_t iterations,
                        const float* scales, int32_t window, int32_t guard, void* stream,
                        uint64_t* tape) {
+  return tc_adjoint_forward_conv(TC_CONVENTION_REFERENCE, adj, n_cb, cbs, llr_len, llr, post_len,
+                                 posterior, iterations, scales, window, guard, stream, tape);
+}
+
+int tc_adjoint_forward_conv(int convention, tc_adjoint* adj, size_t n_cb,
+                            const tc_code_block* cbs, size_t llr_len, const float* llr,
+                            size_t post_len, float* posterior, uint32_t iterations,
+                            const float* scales, int32_t window, int32_t guard, void* stream,
+                            uint64_t* tape) {
   return guarded([&] {
     need(adj != nullptr && tape != nullptr, "null pointer");
     need(n_cb > 0 && cbs && llr && posterior, "null pointer or no code blocks");
@@ -554,6 +563,7 @@ int tc_adjoint_forward(tc_adjoint* adj, size_t n_cb, const tc_code_block* cbs, s
     rq.window = window;
     rq.guard = guard;
     rq.stream = stream;
+    rq.std3gpp = convention_of(convention) == tcb::Convention::Std3gpp;
     *tape = adj->impl.forward(rq);
   });
 }
