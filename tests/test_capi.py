@@ -80,3 +80,25 @@ def test_decoder_without_device_fails_loudly(tc):
         tc.Decoder(0)
     with pytest.raises(tc.InvalidArgument):
         tc.decode_transport_block(tc.LteTurboCodecParams(), None, tc.DecoderBackend.CpuReference)
+
+
+def test_header_is_plain_c(tc, tmp_path):
+    """include/turbo_b200.h compiles as C99 with -pedantic -Werror, and a C program linked to
+    libturbo_b200.so calls the CPU-side entry points (36.212 CRC check value, option defaults,
+    segmentation sizes, QPP, encoder, error status); its view of tc_decode_options has the
+    size the Python binding uses."""
+    import shutil
+
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc is not available")
+    lib_dir = os.path.join(ROOT, "turbo_cpp_b200", "lib")
+    exe = str(tmp_path / "c_api_check")
+    r = subprocess.run(["gcc", "-std=c99", "-pedantic", "-Wall", "-Wextra", "-Werror",
+                        "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "cpp", "c_api_check.c"), "-o", exe,
+                        "-L", lib_dir, "-lturbo_b200", f"-Wl,-rpath,{lib_dir}"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.split() == ["c", "api", "ok", str(C.sizeof(tc._Options))]
