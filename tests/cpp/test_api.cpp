@@ -2,7 +2,10 @@
 // segmentation, transport-block round trips through every GPU backend) run against the C++ API
 // of this library (include/turbo_b200.hpp), plus checks of what that API adds.  The CPU
 // decoder of the reference, which those cases compare the GPU posteriors with, is the oracle
-// (oracle/turbo_oracle.c, bitwise equal to it).  Parity bar: |gpu - cpu| <= 1e-3 max(|cpu|, 1).
+// (oracle/turbo_oracle.c, bitwise equal to it).  Parity bar: |gpu - cpu| <= 1e-3 max(|cpu|, 1),
+// and on the reference's own noise-free round trips (±8 LLRs) a tighter 2e-5 max(|cpu|, 1):
+// the same exact Log-MAP in other float arithmetic agrees there to ~1.5e-6 (a few ulps of
+// posteriors up to ~640; the reference's own Stage-1 check asks 2e-5 absolute, about one ulp).
 //
 //   test_api cpu   -- codec cases only (no GPU)
 //   test_api gpu   -- codec and decoder cases
@@ -246,7 +249,7 @@ void roundtrip_case(std::size_t tbs, std::size_t a, std::size_t c, bool g_from_b
     for (float v : *dec.posterior_llr) finite &= std::isfinite(v);
     expect(finite, tag + ": finite posterior");
     const double err = rel_err(*dec.posterior_llr, cpu);
-    expect(err <= 1e-3, tag + ": posterior vs CPU decoder " + std::to_string(err));
+    expect(err <= 2e-5, tag + ": posterior vs CPU decoder " + std::to_string(err));
     for (bool ok : dec.code_block_crc_ok) expect(ok, tag + ": code block CRC");
   }
   // tile8 entry point: hard decisions equal the encoded block
