@@ -592,8 +592,7 @@ uint64_t Adjoint::forward(const AdjointRequest& rq) {
   const uint16_t* dperm = dec_.perm_table();
   const uint16_t* dinv = dec_.inv_table();
   // sys_i and tape slot 0 (the first a-priori, zero)
-  setup_kernel<<<static_cast<unsigned>((work + 255) / 256), 256, 0, st>>>(
-      dcbs, dstart, static_cast<int>(n), work, rq.llr, dperm, sysi, tape);
+  launch_setup(dcbs, static_cast<int>(n), rq.llr, dperm, sysi, tape, st);
   ok(cudaGetLastError(), "setup launch");
   launches_ += 1;
   const int blocks = (n_win + kThreads - 1) / kThreads;

@@ -41,23 +41,29 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) siso_plain_kernel(const 
   }
 }
 
-// sys_i[i] = d0[Pi(i)]; E2 = 0 (first a-priori); one thread per (block, position).
-__global__ void setup_kernel(const DevCb* __restrict__ cbs, const int64_t* __restrict__ cb_start,
-                             int n_cb, int64_t total, const float* __restrict__ llr,
+// sys_i[i] = d0[Pi(i)]; E2 = 0 (first a-priori).  The grid's y index walks the code blocks and
+// its x index the positions of one block (24 x 256 threads cover the largest K), so no thread
+// has to search for its block.
+constexpr int kSetupThreads = 256;
+constexpr int kSetupBlocksPerCb = (6144 + kSetupThreads - 1) / kSetupThreads;
+__global__ void setup_kernel(const DevCb* __restrict__ cbs, int n_cb, const float* __restrict__ llr,
                              const uint16_t* __restrict__ perm, float* __restrict__ sys_i,
                              float* __restrict__ e2) {
-  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= total) return;
-  // binary search of the owning block
-  int lo = 0, hi = n_cb - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (cb_start[mid] <= i) lo = mid; else hi = mid - 1;
+  const int p = blockIdx.x * kSetupThreads + threadIdx.x;
+  for (int c = blockIdx.y; c < n_cb; c += gridDim.y) {
+    const DevCb cb = cbs[c];
+    if (p < cb.k) {
+      sys_i[cb.work + p] = llr[cb.llr + perm[cb.tab + p]];
+      e2[cb.work + p] = 0.0f;
+    }
   }
-  const DevCb cb = cbs[lo];
-  const int64_t p = i - cb_start[lo];
-  sys_i[cb.work + p] = llr[cb.llr + perm[cb.tab + p]];
-  e2[cb.work + p] = 0.0f;
+}
+
+inline void launch_setup(const DevCb* cbs, int n_cb, const float* llr, const uint16_t* perm,
+                         float* sys_i, float* e2, cudaStream_t st) {
+  if (n_cb <= 0) return;
+  const dim3 grid(kSetupBlocksPerCb, static_cast<unsigned>(n_cb < 65535 ? n_cb : 65535));
+  setup_kernel<<<grid, kSetupThreads, 0, st>>>(cbs, n_cb, llr, perm, sys_i, e2);
 }
 
 // CRC24B early stop (lte_turbo.cpp:792-804): hard decisions (>= 0 -> 1) of bits

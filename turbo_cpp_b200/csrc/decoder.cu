@@ -175,7 +175,7 @@ Decoder::~Decoder() {
   }
   workers_.clear();  // each waits for its own work (cudaFree) and releases its buffers
   if (stream_) cudaStreamDestroy(static_cast<cudaStream_t>(stream_));
-  for (DeviceBuffer* b : {&d_perm_, &d_inv_, &d_xpow_, &d_xpow_std_, &d_xpow_a_std_, &d_cbs_, &d_wincb_, &d_start_, &d_llr_,
+  for (DeviceBuffer* b : {&d_perm_, &d_inv_, &d_xpow_, &d_xpow_std_, &d_xpow_a_std_, &d_cbs_, &d_wincb_, &d_llr_,
                           &d_sysi_, &d_e1i_, &d_e2_, &d_post_, &d_seed_, &d_done_, &d_iters_,
                           &d_crc_, &d_ckpt_, &d_tasks_, &d_queue_, &d_rm_, &d_e_llr_, &d_d012_,
                           &d_tbpost_, &d_tbbits_, &d_tbok_, &d_cbok_, &d_tbiters_, &d_tb_,
@@ -550,7 +550,6 @@ void Decoder::decode_plain(const DecodeRequest& rq) {
   const int guard = rq.guard < 0 ? kDefaultGuard : rq.guard;
   if (guard % kGroup != 0) throw InvalidArgument("guard must be a multiple of 8");
   std::vector<DevCb> cbs(n);
-  std::vector<int64_t> start(n);
   std::vector<int32_t> wincb;
   int64_t work = 0;
   int max_ckpt = 0;
@@ -577,7 +576,6 @@ void Decoder::decode_plain(const DecodeRequest& rq) {
     d.llr = rq.cbs[i].llr_offset;
     d.work = work;
     d.out = rq.cbs[i].out_offset;
-    start[i] = work;
     work += k;
     max_ckpt = std::max(max_ckpt, d.window / kSub);
     for (int w = 0; w < d.nwin; ++w) wincb.push_back(static_cast<int32_t>(i));
@@ -592,7 +590,6 @@ void Decoder::decode_plain(const DecodeRequest& rq) {
   // ---- device buffers ----
   DevCb* dcbs = grow<DevCb>(d_cbs_, n);
   int32_t* dwin = grow<int32_t>(d_wincb_, n_win);
-  int64_t* dstart = grow<int64_t>(d_start_, n);
   float* sysi = grow<float>(d_sysi_, work);
   float* e1i = grow<float>(d_e1i_, work);
   float* e2 = grow<float>(d_e2_, work);
@@ -617,7 +614,6 @@ void Decoder::decode_plain(const DecodeRequest& rq) {
 
   upload(dcbs, cbs.data(), n * sizeof(DevCb), st);
   upload(dwin, wincb.data(), n_win * sizeof(int32_t), st);
-  upload(dstart, start.data(), n * sizeof(int64_t), st);
   check(cudaMemsetAsync(seeds, 0, static_cast<size_t>(n_win) * 16 * 4 * sizeof(float), st), "zero seeds");
   init_flags_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(
       static_cast<int>(n), done, iters, rq.max_iterations);
@@ -626,8 +622,7 @@ void Decoder::decode_plain(const DecodeRequest& rq) {
   const uint16_t* dperm = static_cast<const uint16_t*>(d_perm_.ptr);
   const uint16_t* dinv = static_cast<const uint16_t*>(d_inv_.ptr);
   timing_.launches += 3;  // init, setup, finish
-  setup_kernel<<<static_cast<unsigned>((work + 255) / 256), 256, 0, st>>>(
-      dcbs, dstart, static_cast<int>(n), work, llr, dperm, sysi, e2);
+  launch_setup(dcbs, static_cast<int>(n), llr, dperm, sysi, e2, st);
   check(cudaGetLastError(), "setup launch");
 
   const int blocks = (n_win + kThreads - 1) / kThreads;
@@ -744,7 +739,6 @@ void Decoder::decode_persistent(const DecodeRequest& rq) {
 
   // ---- per block: at most 32 windows of >= `target` steps (a multiple of 8, >= guard) ----
   std::vector<DevCb> cbs(n);
-  std::vector<int64_t> start(n);
   int64_t work = 0;
   int max_ckpt = 0;
   for (size_t i = 0; i < n; ++i) {
@@ -773,7 +767,6 @@ void Decoder::decode_persistent(const DecodeRequest& rq) {
     d.llr = rq.cbs[i].llr_offset;
     d.work = work;
     d.out = rq.cbs[i].out_offset;
-    start[i] = work;
     work += k;
     max_ckpt = std::max(max_ckpt, d.window / kSub);
   }
@@ -804,7 +797,6 @@ void Decoder::decode_persistent(const DecodeRequest& rq) {
   // ---- device buffers ----
   DevCb* dcbs = grow<DevCb>(d_cbs_, n);
   int32_t* dwin = grow<int32_t>(d_wincb_, n_win);
-  int64_t* dstart = grow<int64_t>(d_start_, n);
   int32_t* dtasks = grow<int32_t>(d_tasks_, tasks.size());
   int* dqueue = grow<int>(d_queue_, 2 + static_cast<size_t>(n_tasks));  // queue, error, progress
   float* sysi = grow<float>(d_sysi_, work);
@@ -828,7 +820,6 @@ void Decoder::decode_persistent(const DecodeRequest& rq) {
   }
   upload(dcbs, cbs.data(), n * sizeof(DevCb), st);
   upload(dwin, wincb.data(), n_win * sizeof(int32_t), st);
-  upload(dstart, start.data(), n * sizeof(int64_t), st);
   upload(dtasks, tasks.data(), tasks.size() * sizeof(int32_t), st);
   check(cudaMemsetAsync(dqueue, 0, (2 + static_cast<size_t>(n_tasks)) * sizeof(int), st),
         "zero queue");
@@ -836,9 +827,8 @@ void Decoder::decode_persistent(const DecodeRequest& rq) {
         "zero seeds");
   init_flags_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(
       static_cast<int>(n), done, iters, rq.max_iterations);
-  setup_kernel<<<static_cast<unsigned>((work + 255) / 256), 256, 0, st>>>(
-      dcbs, dstart, static_cast<int>(n), work, llr, static_cast<const uint16_t*>(d_perm_.ptr),
-      sysi, e2);
+  launch_setup(dcbs, static_cast<int>(n), llr, static_cast<const uint16_t*>(d_perm_.ptr), sysi,
+               e2, st);
   check(cudaGetLastError(), "set-up launch");
 
   PersistArgs a{};

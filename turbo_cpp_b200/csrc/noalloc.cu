@@ -129,7 +129,6 @@ void decode_noalloc(const DecodeRequest& rq, size_t* bytes_needed) {
 
   // ---- layout (as the decoder object's plain schedule) ----
   std::vector<DevCb> cbs(n);
-  std::vector<int64_t> start(n);
   std::vector<int32_t> wincb;
   int64_t work = 0;
   int max_ckpt = 0;
@@ -156,7 +155,6 @@ void decode_noalloc(const DecodeRequest& rq, size_t* bytes_needed) {
     d.llr = rq.cbs[i].llr_offset;
     d.work = work;
     d.out = rq.cbs[i].out_offset;
-    start[i] = work;
     work += k;
     max_ckpt = std::max(max_ckpt, d.window / kSub);
     for (int w = 0; w < d.nwin; ++w) wincb.push_back(static_cast<int32_t>(i));
@@ -167,7 +165,6 @@ void decode_noalloc(const DecodeRequest& rq, size_t* bytes_needed) {
   Carve c{ds.scratch};
   DevCb* dcbs = c.take<DevCb>(n);
   int32_t* dwin = c.take<int32_t>(n_win);
-  int64_t* dstart = c.take<int64_t>(n);
   float* sysi = c.take<float>(work);
   float* e1i = c.take<float>(work);
   float* e2 = c.take<float>(work);
@@ -187,14 +184,11 @@ void decode_noalloc(const DecodeRequest& rq, size_t* bytes_needed) {
   ok(cudaMemcpyAsync(dcbs, cbs.data(), n * sizeof(DevCb), cudaMemcpyHostToDevice, st), "copy cbs");
   ok(cudaMemcpyAsync(dwin, wincb.data(), n_win * sizeof(int32_t), cudaMemcpyHostToDevice, st),
      "copy windows");
-  ok(cudaMemcpyAsync(dstart, start.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, st),
-     "copy starts");
   ok(cudaMemsetAsync(seeds, 0, static_cast<size_t>(n_win) * 16 * 4 * sizeof(float), st),
      "zero seeds");
   init_flags_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(
       static_cast<int>(n), done, iters, rq.max_iterations);
-  setup_kernel<<<static_cast<unsigned>((work + 255) / 256), 256, 0, st>>>(
-      dcbs, dstart, static_cast<int>(n), work, rq.llr, ds.perm, sysi, e2);
+  launch_setup(dcbs, static_cast<int>(n), rq.llr, ds.perm, sysi, e2, st);
   ok(cudaGetLastError(), "set-up launch");
   const int blocks = (n_win + kThreads - 1) / kThreads;
   const size_t slab = static_cast<size_t>(n_win) * 16;
