@@ -380,9 +380,7 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
 
 struct CombineIo {
   const DevCb* cbs;
-  const int64_t* start;   // first work position of each block
   int n_cb;
-  int64_t total;
   int guard;
   const float* own_sa;
   const float* own_par;
@@ -394,19 +392,10 @@ struct CombineIo {
   float* ge_out;           // upper: d/d e2 of the previous iteration; lower: d/d e1 (natural)
 };
 
-// One thread per position of the SISO's order: own + neighbours' warm-up gradients, then
+// Position p of code block cb in the SISO's order: own + neighbours' warm-up gradients, then
 // d0/d1/d2 and the adjoint of the a-priori (the other SISO's scaled extrinsic).
-template <bool LOWER, bool LAST, bool STD = false>
-__global__ void adj_combine_kernel(CombineIo c) {
-  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= c.total) return;
-  int lo_c = 0, hi_c = c.n_cb - 1;
-  while (lo_c < hi_c) {
-    const int mid = (lo_c + hi_c + 1) >> 1;
-    if (c.start[mid] <= i) lo_c = mid; else hi_c = mid - 1;
-  }
-  const DevCb cb = c.cbs[lo_c];
-  const int p = static_cast<int>(i - c.start[lo_c]);
+template <bool LOWER, bool LAST, bool STD>
+__device__ __forceinline__ void combine_position(const CombineIo& c, const DevCb& cb, int p) {
   const int W = cb.window, G = c.guard, K = cb.k;
   const int w = p / W, lo = w * W;
   float sa = c.own_sa[cb.work + p], par = c.own_par[cb.work + p];
@@ -467,23 +456,31 @@ __global__ void adj_combine_kernel(CombineIo c) {
   }
 }
 
+// One thread per position; as setup_kernel, the grid's y index walks the code blocks and its x
+// index (kSetupBlocksPerCb x kSetupThreads) the positions of one block.
+template <bool LOWER, bool LAST, bool STD = false>
+__global__ void adj_combine_kernel(CombineIo c) {
+  const int p = blockIdx.x * kSetupThreads + threadIdx.x;
+  for (int i = blockIdx.y; i < c.n_cb; i += gridDim.y) {
+    const DevCb cb = c.cbs[i];
+    if (p < cb.k) combine_position<LOWER, LAST, STD>(c, cb, p);
+  }
+}
+
 // grad_llr: d0 gets d loss / d posterior (posterior = Ls + e1 + e2); ge2 = d loss / d e2 of the
 // last iteration (work layout).  grad_llr was zeroed before.
-__global__ void adj_init_kernel(const DevCb* __restrict__ cbs, const int64_t* __restrict__ start,
-                                int n_cb, int64_t total, const float* __restrict__ grad_post,
-                                float* __restrict__ grad_llr, float* __restrict__ ge2) {
-  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= total) return;
-  int lo = 0, hi = n_cb - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (start[mid] <= i) lo = mid; else hi = mid - 1;
+__global__ void adj_init_kernel(const DevCb* __restrict__ cbs, int n_cb,
+                                const float* __restrict__ grad_post, float* __restrict__ grad_llr,
+                                float* __restrict__ ge2) {
+  const int p = blockIdx.x * kSetupThreads + threadIdx.x;
+  for (int i = blockIdx.y; i < n_cb; i += gridDim.y) {
+    const DevCb cb = cbs[i];
+    if (p < cb.k) {
+      const float gp = grad_post[cb.out + p];
+      grad_llr[cb.llr + p] = gp;
+      ge2[cb.work + p] = gp;
+    }
   }
-  const DevCb cb = cbs[lo];
-  const int64_t p = i - start[lo];
-  const float gp = grad_post[cb.out + p];
-  grad_llr[cb.llr + p] = gp;
-  ge2[cb.work + p] = gp;
 }
 
 // grad_scales[j] = sum over windows of part[j][window], in a fixed order (one block per j).
@@ -511,7 +508,7 @@ T* reserve(DeviceBuffer& b, size_t count) {
 }  // namespace
 
 Adjoint::~Adjoint() {
-  for (DeviceBuffer* b : {&d_cbs_, &d_wincb_, &d_start_, &d_sysi_, &d_tape_, &d_seeds_, &d_ckpt_,
+  for (DeviceBuffer* b : {&d_cbs_, &d_wincb_, &d_sysi_, &d_tape_, &d_seeds_, &d_ckpt_,
                           &d_own_, &d_guard_, &d_tail_, &d_part_, &d_ge2_, &d_ga1_})
     b->release();
 }
@@ -532,7 +529,6 @@ uint64_t Adjoint::forward(const AdjointRequest& rq) {
   if (window_req % kGroup != 0) throw InvalidArgument("window must be a multiple of 8");
 
   std::vector<DevCb> cbs_(n);
-  std::vector<int64_t> start(n);
   std::vector<int32_t> wincb;
   int64_t work = 0;
   int max_window = 0;
@@ -556,7 +552,6 @@ uint64_t Adjoint::forward(const AdjointRequest& rq) {
     d.llr = rq.cbs[i].llr_offset;
     d.work = work;
     d.out = rq.cbs[i].out_offset;
-    start[i] = work;
     work += k;
     max_window = std::max(max_window, d.window);
     for (int w = 0; w < d.nwin; ++w) wincb.push_back(static_cast<int32_t>(i));
@@ -579,7 +574,6 @@ uint64_t Adjoint::forward(const AdjointRequest& rq) {
 
   DevCb* dcbs = reserve<DevCb>(d_cbs_, n);
   int32_t* dwin = reserve<int32_t>(d_wincb_, n_win);
-  int64_t* dstart = reserve<int64_t>(d_start_, n);
   float* sysi = reserve<float>(d_sysi_, work);
   float* tape = reserve<float>(d_tape_, static_cast<size_t>(2 * I + 1) * work);
   const size_t slab = static_cast<size_t>(n_win) * 16;
@@ -587,7 +581,6 @@ uint64_t Adjoint::forward(const AdjointRequest& rq) {
   float4* ckpt = reserve<float4>(d_ckpt_, static_cast<size_t>(n_win) * 2 * ckpt_fwd_);
   ok(cudaMemcpyAsync(dcbs, cbs_.data(), n * sizeof(DevCb), cudaMemcpyHostToDevice, st), "copy descriptors");
   ok(cudaMemcpyAsync(dwin, wincb.data(), n_win * sizeof(int32_t), cudaMemcpyHostToDevice, st), "copy descriptors");
-  ok(cudaMemcpyAsync(dstart, start.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, st), "copy descriptors");
   ok(cudaMemsetAsync(seeds, 0, 2 * slab * sizeof(float), st), "zero seeds");
   const uint16_t* dperm = dec_.perm_table();
   const uint16_t* dinv = dec_.inv_table();
@@ -643,16 +636,15 @@ void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr
   float4* ckpt = reserve<float4>(d_ckpt_, static_cast<size_t>(n_win) * 4 * ckpt_bwd_);
   const DevCb* dcbs = static_cast<const DevCb*>(d_cbs_.ptr);
   const int32_t* dwin = static_cast<const int32_t*>(d_wincb_.ptr);
-  const int64_t* dstart = static_cast<const int64_t*>(d_start_.ptr);
   const float* sysi = static_cast<const float*>(d_sysi_.ptr);
   const float* tape = static_cast<const float*>(d_tape_.ptr);
   const float* seeds = static_cast<const float*>(d_seeds_.ptr);
   const uint16_t* dperm = dec_.perm_table();
   const int n = static_cast<int>(n_cb_);
-  const unsigned pos_blocks = static_cast<unsigned>((work + 255) / 256);
+  const dim3 pos_blocks(kSetupBlocksPerCb, static_cast<unsigned>(n < 65535 ? n : 65535));
 
   ok(cudaMemsetAsync(grad_llr, 0, llr_len_ * sizeof(float), st), "zero grad_llr");
-  adj_init_kernel<<<pos_blocks, 256, 0, st>>>(dcbs, dstart, n, work, grad_post, grad_llr, ge2);
+  adj_init_kernel<<<pos_blocks, kSetupThreads, 0, st>>>(dcbs, n, grad_post, grad_llr, ge2);
   ok(cudaGetLastError(), "adjoint init launch");
   launches_ += 1;
   const int blocks = (n_win + kAdjThreads - 1) / kAdjThreads;
@@ -678,21 +670,21 @@ void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr
       siso_adjoint_kernel<false, 2><<<blocks, kAdjThreads, 0, st>>>(dcbs, dwin, n_win, io);
     }
     ok(cudaGetLastError(), "SISO adjoint launch");
-    CombineIo c{dcbs, dstart, n, work, G, own, own + work, guard_g, tail_g, dperm, grad_post,
-                grad_llr, lower ? ga1 : ge2};
+    CombineIo c{dcbs, n, G, own, own + work, guard_g, tail_g, dperm, grad_post, grad_llr,
+                lower ? ga1 : ge2};
     if (std3gpp_) {
       if (lower && last)
-        adj_combine_kernel<true, true, true><<<pos_blocks, 256, 0, st>>>(c);
+        adj_combine_kernel<true, true, true><<<pos_blocks, kSetupThreads, 0, st>>>(c);
       else if (lower)
-        adj_combine_kernel<true, false, true><<<pos_blocks, 256, 0, st>>>(c);
+        adj_combine_kernel<true, false, true><<<pos_blocks, kSetupThreads, 0, st>>>(c);
       else
-        adj_combine_kernel<false, false, true><<<pos_blocks, 256, 0, st>>>(c);
+        adj_combine_kernel<false, false, true><<<pos_blocks, kSetupThreads, 0, st>>>(c);
     } else if (lower && last) {
-      adj_combine_kernel<true, true><<<pos_blocks, 256, 0, st>>>(c);
+      adj_combine_kernel<true, true><<<pos_blocks, kSetupThreads, 0, st>>>(c);
     } else if (lower) {
-      adj_combine_kernel<true, false><<<pos_blocks, 256, 0, st>>>(c);
+      adj_combine_kernel<true, false><<<pos_blocks, kSetupThreads, 0, st>>>(c);
     } else {
-      adj_combine_kernel<false, false><<<pos_blocks, 256, 0, st>>>(c);
+      adj_combine_kernel<false, false><<<pos_blocks, kSetupThreads, 0, st>>>(c);
     }
     ok(cudaGetLastError(), "adjoint combine launch");
     launches_ += 3;

@@ -67,7 +67,7 @@ class Adjoint {
   bool std3gpp_ = false;
   std::vector<float> scales_;
   const float* llr_ = nullptr;
-  DeviceBuffer d_cbs_, d_wincb_, d_start_, d_sysi_, d_tape_, d_seeds_, d_ckpt_;
+  DeviceBuffer d_cbs_, d_wincb_, d_sysi_, d_tape_, d_seeds_, d_ckpt_;
   DeviceBuffer d_own_, d_guard_, d_tail_, d_part_, d_ge2_, d_ga1_;
 };
 
