@@ -284,8 +284,13 @@ TC_API int tc_decode_transport_blocks(tc_decoder* dec, size_t n_tb, const tc_tra
  * each GPU that loads it until the library is unloaded); a request that needs more is refused
  * with TC_ERR_CAPACITY before any work is enqueued (*scratch_bytes, when given, receives the
  * bytes the request needs; about 135 KB per K=6144 code block, i.e. ~240 such blocks).  The
- * first call on a device copies constant tables synchronously: make it before capturing a
- * stream.  All calls on a device share the array; calls that overlap on the GPU race. */
+ * first call on a device copies constant tables synchronously: make it before any stream
+ * capture begins.  Every call copies its block descriptors from memory that lives only for the
+ * call, so a call made while its stream is capturing is refused (TC_ERR_INVALID_ARGUMENT).
+ * Those tables are uploaded once per device and process: after cudaDeviceReset the entry point
+ * must not be used again in that process (a module reloaded at another address is detected and
+ * set up again; one reloaded at the same address is not).  All calls on a device share the
+ * array; calls that overlap on the GPU race. */
 TC_API int tc_decode_noalloc(size_t n_cb, const tc_code_block* cbs, size_t llr_len,
                              const float* llr, size_t post_len, float* posterior,
                              uint8_t* crc_ok, uint32_t* iterations_used,

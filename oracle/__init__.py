@@ -27,8 +27,11 @@ CRC24A, CRC24B, CRC16, CRC8 = 0, 1, 2, 3
 CRC_LEN = {CRC24A: 24, CRC24B: 24, CRC16: 16, CRC8: 8}
 
 
-def build(ref_root: str = "/root/reference") -> None:
-    """Compile liboracle.so and, when the reference sources exist, _ref/libturbo_ref.so."""
+def build(ref_root: str | None = None) -> None:
+    """Compile liboracle.so and, when the reference sources are given (`ref_root`, else the
+    TURBO_CPP_REF environment variable) and exist, _ref/libturbo_ref.so.  Without them the
+    reference library is skipped with a notice (a prebuilt one is kept)."""
+    ref_root = ref_root or os.environ.get("TURBO_CPP_REF", "")
     subprocess.run(["make", "-s", "-C", HERE, "all", f"REF={ref_root}"], check=True)
 
 

@@ -6,7 +6,9 @@ allocator, a plug-in handed only its buffers); all of its scratch comes from a f
 library.  These tests call it through the C ABI and compare it with tc_decode, the entry point
 that allocates, at the tolerance the other decoder tests use, on two calls in a row (the second
 with other inputs and options, so leftovers of the first call in the shared array would show),
-and check that an oversized request is refused.  This file is collected last on purpose.
+check that an oversized request is refused, that a call leaves the device's free memory
+unchanged, and that a call made while its stream is capturing is refused.  This file is
+collected last on purpose.
 """
 from __future__ import annotations
 
@@ -78,3 +80,56 @@ def test_noalloc_refuses_oversized_requests(tc):
     assert need.value > SCRATCH_LIMIT and b"scratch" in lib.tc_last_error()
     torch.cuda.synchronize()
     assert torch.count_nonzero(post).item() == 0  # nothing was launched
+
+
+def test_noalloc_allocates_no_device_memory(tc):
+    """After a first call (which sets the device up and, with the same options, loads every
+    kernel the second call runs), a larger call changes the device's free memory by nothing: all
+    of its scratch is the library's own array."""
+    import torch
+
+    stream = torch.cuda.Stream()
+    small = [1024, 40]
+    llr, _ = awgn_blocks(tc, small, 0.8, seed=320)
+    _noalloc(tc, small, [0, 0], llr, tc.DecodeOptions(8, True), stream)
+    ks = [6144] * 48 + [2048, 40]
+    llr, _ = awgn_blocks(tc, ks, 0.8, seed=321)
+    lib = tc.load_library()
+    cbs, llr_len, post_len = tc.Decoder.layout(ks)
+    x = torch.from_numpy(llr).cuda()
+    post = torch.empty(post_len, dtype=torch.float32, device="cuda")
+    ok = torch.zeros(len(ks), dtype=torch.uint8, device="cuda")
+    it = torch.zeros(len(ks), dtype=torch.int32, device="cuda")
+    opt, _keep = tc.Decoder._opts(tc.DecodeOptions(8, True), tc.MEM_DEVICE, stream.cuda_stream)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    rc = lib.tc_decode_noalloc(len(ks), C.addressof(cbs), llr_len, x.data_ptr(), post_len,
+                               post.data_ptr(), ok.data_ptr(), it.data_ptr(), C.addressof(opt),
+                               None)
+    assert rc == 0, lib.tc_last_error()
+    stream.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert np.all(np.isfinite(post.cpu().numpy()))
+
+
+def test_noalloc_refuses_a_capturing_stream(tc):
+    """The descriptors are copied from call-local host memory, so a call on a stream that is
+    being captured is refused before anything is enqueued (the capture stays valid)."""
+    import torch
+
+    lib = tc.load_library()
+    ks = [1024]
+    cbs, llr_len, post_len = tc.Decoder.layout(ks)
+    x = torch.zeros(llr_len, dtype=torch.float32, device="cuda")
+    post = torch.zeros(post_len, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    opt, _ = tc.Decoder._opts(tc.DecodeOptions(8), tc.MEM_DEVICE, stream.cuda_stream)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        rc = lib.tc_decode_noalloc(len(ks), C.addressof(cbs), llr_len, x.data_ptr(), post_len,
+                                   post.data_ptr(), None, None, C.addressof(opt), None)
+    assert rc == 1  # TC_ERR_INVALID_ARGUMENT
+    assert b"captured" in lib.tc_last_error()
+    del graph

@@ -59,12 +59,20 @@ void ok(cudaError_t e, const char* what) {
 
 // First call on a device: symbol addresses and the constant tables (QPP permutations and
 // x^j mod g_CRC24B).  This uses synchronous copies, so the first call on each device must not
-// be made while a stream is being captured.
+// be made while a stream is being captured.  Later calls re-read one symbol address (a cheap
+// lookup) and redo the set-up when the module was loaded again at another address.  A device
+// reset that reloads the module at the same address is not detected: the tables are then gone,
+// which the header states as a limit.
 const DeviceState& setup(int device) {
   std::lock_guard<std::mutex> lock(g_setup_mu);
   if (device < 0 || device >= kMaxDevices) throw InvalidArgument("device ordinal out of range");
   DeviceState& d = g_state[device];
-  if (d.ready) return d;
+  if (d.ready) {
+    uint16_t* perm = nullptr;
+    ok(cudaGetSymbolAddress(reinterpret_cast<void**>(&perm), g_perm), "table address");
+    if (perm == d.perm) return d;
+    d.ready = false;
+  }
   ok(cudaGetSymbolAddress(reinterpret_cast<void**>(&d.scratch), g_scratch), "scratch address");
   ok(cudaGetSymbolAddress(reinterpret_cast<void**>(&d.perm), g_perm), "table address");
   ok(cudaGetSymbolAddress(reinterpret_cast<void**>(&d.inv), g_inv), "table address");
@@ -119,8 +127,15 @@ struct Carve {
 void decode_noalloc(const DecodeRequest& rq, size_t* bytes_needed) {
   int device = 0;
   ok(cudaGetDevice(&device), "cudaGetDevice");
-  const DeviceState& ds = setup(device);
   cudaStream_t st = static_cast<cudaStream_t>(rq.stream);
+  // The block descriptors below are copied from host memory that lives only for this call, and
+  // the first call's set-up copies synchronously; neither may be recorded into a graph.
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  ok(cudaStreamIsCapturing(st, &capture), "cudaStreamIsCapturing");
+  if (capture != cudaStreamCaptureStatusNone)
+    throw InvalidArgument("tc_decode_noalloc was called while its stream is being captured; its "
+                          "descriptor copies read memory that lives only for the call");
+  const DeviceState& ds = setup(device);
   const size_t n = rq.n_cb;
   if (reinterpret_cast<uintptr_t>(rq.llr) % 16 != 0)
     throw InvalidArgument("the LLR buffer must be 16-byte aligned");
