@@ -114,3 +114,36 @@ def test_scale_gradient_is_the_extrinsic_correlation(oracle, tc):
     _, gp = _bce(p0, bits)
     _, _, _, g_s = oracle.adj_vjp(k, llr, s0, grad_post=gp)
     assert abs(g_s[3] - float(np.dot(gp, p1 - p0))) <= 1e-9 * max(1.0, abs(g_s[3]))
+
+
+@pytest.mark.parametrize("k,window,guard,iters,bound", [(1024, 64, 32, 6, 2e-3),
+                                                        (1024, 128, 96, 6, 1e-6)])
+def test_frozen_seed_gradient_vs_true_gradient(oracle, tc, k, window, guard, iters, bound):
+    """The differentiated function treats the next-iteration seeds as constants.  Here the true
+    gradient of the windowed decoder -- seeds recomputed by every perturbed run, i.e. not frozen
+    -- is taken by FP64 central differences and compared with the frozen-seed adjoint.  Measured
+    worst relative error over the 12 scales and 64 sampled LLRs: 5.6e-4 with window 64 and guard
+    32 (the training schedule), 1.5e-8 with window 128 and guard 96, where the seeds barely move
+    the posteriors; the directions agree to cosine similarity 1 - 1e-9 or better."""
+    llr, bits, scales = _case(tc, k, 0.6, k + window, iters)
+    post, seeds, _, _ = oracle.adj_vjp(k, llr, scales, window, guard)
+    _, gp = _bce(post, bits)
+    _, _, g_llr, g_s = oracle.adj_vjp(k, llr, scales, window, guard, grad_post=gp,
+                                      frozen_seeds=seeds)
+
+    def loss(l, s):  # seeds follow the perturbed run
+        return _bce(oracle.adj_vjp(k, l, s, window, guard)[0], bits)[0]
+
+    fd_s = np.array([(loss(llr, scales + H * e) - loss(llr, scales - H * e)) / (2 * H)
+                     for e in np.eye(scales.size)])
+    pos = np.random.default_rng(k).choice(3 * (k + 4), 64, replace=False)
+    fd_l = np.empty(pos.size)
+    for j, i in enumerate(pos):
+        e = np.zeros_like(llr)
+        e[i] = H
+        fd_l[j] = (loss(llr + e, scales) - loss(llr - e, scales)) / (2 * H)
+    err_s = np.abs(fd_s - g_s).max() / np.abs(fd_s).max()
+    err_l = np.abs(fd_l - g_llr[pos]).max() / np.abs(fd_l).max()
+    cos_s = np.dot(fd_s, g_s) / np.linalg.norm(fd_s) / np.linalg.norm(g_s)
+    assert err_s < bound and err_l < bound, (err_s, err_l)
+    assert cos_s > 1.0 - 1e-6

@@ -22,9 +22,9 @@ from . import (LteTurboCodecParams, awgn_code_blocks, awgn_llr, encode_transport
                qpp_interleaver_table, random_bits)
 
 
-def config3_transport_blocks(n_tb: int, seed: int):
+def config3_transport_blocks(n_tb: int, seed: int, llr_seed: int | None = None):
     """Returns (tbs list of (TBS, C), blocks list of (K, F, E, rv), rate-matched LLRs, info bits
-    per TB, Eb/N0 per TB)."""
+    per TB, Eb/N0 per TB).  `llr_seed` draws other channel noise for the same blocks."""
     rng = np.random.default_rng(seed)
     tbs, blocks, llrs, bits_out, ebs = [], [], [], [], []
     for t in range(n_tb):
@@ -37,7 +37,7 @@ def config3_transport_blocks(n_tb: int, seed: int):
         enc = encode_transport_block(p, bits)
         rm = np.concatenate([b.rate_matched_bits for b in enc.code_blocks])
         sigma2 = 1.0 / (2.0 * (tbs_bits / g) * 10 ** (eb / 10.0))
-        llrs.append(awgn_llr(seed * 7919 + t, rm, sigma2))
+        llrs.append(awgn_llr((seed if llr_seed is None else llr_seed) * 7919 + t, rm, sigma2))
         for b in enc.code_blocks:
             d = b.descriptor
             blocks.append((d.k_r, d.filler_count, d.e_r, 0))
