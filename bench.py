@@ -297,7 +297,7 @@ def config3_figure(tc, dev, stream, iters):
 
     tbs, blocks, e_llr, truth, ebs = config3_transport_blocks(512, seed=33)
     info = sum(t[0] for t in tbs)
-    arr, e_len, _ = tc.Decoder.rm_blocks(blocks)  # descriptors built once, as a receiver would
+    arr, e_len, llr_len = tc.Decoder.rm_blocks(blocks)  # descriptors built once, as a receiver would
     tba = (tc._TransportBlock * len(tbs))()
     first = nbits = 0
     for i, (size, ncb) in enumerate(tbs):
@@ -316,10 +316,23 @@ def config3_figure(tc, dev, stream, iters):
     dcb = torch.zeros(n_cb, dtype=torch.uint8, device="cuda")
     dit = torch.zeros(n_cb, dtype=torch.int32, device="cuda")
     out = {}
-    for name, sched in (("persistent", tc.SCHEDULE_PERSISTENT), ("plain", tc.SCHEDULE_PLAIN)):
+    # the decode request the chain makes (its de-rate-matched code blocks), autotuned once
+    d012 = torch.zeros(llr_len, dtype=torch.float32, device="cuda")
+    dev.derate_device(blocks, dx.data_ptr(), int(e_len), d012.data_ptr(), llr_len,
+                      stream=stream.cuda_stream)
+    cbs, _, post_len = tc.Decoder.layout([b[0] for b in blocks], [b[1] for b in blocks])
+    tpost = torch.empty(post_len, dtype=torch.float32, device="cuda")
+    tuned = dev.autotune(cbs, n_cb, d012.data_ptr(), llr_len, tpost.data_ptr(), post_len,
+                         tc.DecodeOptions(iters, True), stream.cuda_stream)
+    del d012, tpost
+    out["autotune"] = tuned
+    for name, sched, graph in (("autotuned", tc.SCHEDULE_AUTO, True),
+                               ("persistent", tc.SCHEDULE_PERSISTENT, False),
+                               ("plain", tc.SCHEDULE_PLAIN, False)):
         o = tc.DecodeOptions(iters, True, 0, -1, sched)
+        og = tc.DecodeOptions(iters, True, 0, -1, sched, graph=graph)
         hopt, _k1 = dev._opts(o, tc.MEM_HOST)
-        dopt, _k2 = dev._opts(o, tc.MEM_DEVICE, stream.cuda_stream)
+        dopt, _k2 = dev._opts(og, tc.MEM_DEVICE, stream.cuda_stream)
 
         def host_call():
             tc._call("tc_decode_transport_blocks", dev._h, n_tb, ctypes.addressof(tba), n_cb,
@@ -359,6 +372,7 @@ def config3_figure(tc, dev, stream, iters):
         st_dt = (time.perf_counter() - t) / sreps
         for b_, _, _, _ in outs:
             assert np.array_equal(b_.numpy(), hbits.numpy())
+        dev_call()  # with a graph: the capture
         dev_call()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -376,7 +390,10 @@ def config3_figure(tc, dev, stream, iters):
         out[name] = {"value": info / dt / 1e6, "unit": "Mbit/s", "ms": dt * 1e3,
                      "streamed": {"value": info / st_dt / 1e6, "unit": "Mbit/s",
                                   "ms": st_dt * 1e3},
-                     "device_resident": {"value": info / dms / 1e3, "unit": "Mbit/s", "ms": dms},
+                     "device_resident": {"value": info / dms / 1e3, "unit": "Mbit/s", "ms": dms,
+                                         "cuda_graph": graph,
+                                         "schedule": "autotuned" if sched == tc.SCHEDULE_AUTO
+                                         else name},
                      "tb_crc_pass": float(htb.float().mean()), "tb_bit_errors_blocks": tb_err,
                      "mean_iterations": float(hit.float().mean())}
     out["workload"] = (f"{len(tbs)} TBs, TBS ~ U(multiples of 8 in [1000, 97896]) (stand-in for "
@@ -384,7 +401,9 @@ def config3_figure(tc, dev, stream, iters):
                        f"U[0.5,3.0] dB per TB, 8 max iterations, CRC24B early stop; value: host "
                        f"LLRs in, host bits out (pinned, synchronous call); streamed: back-to-back "
                        f"TC_MEM_HOST_ASYNC calls, one sync; device_resident: the same call on "
-                       f"device buffers")
+                       f"device buffers (autotuned: SCHEDULE_AUTO after tc_autotune on the "
+                       f"chain's code blocks, de-rate matching + decode + finish replayed as one "
+                       f"CUDA graph)")
     return out
 
 

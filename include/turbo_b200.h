@@ -146,11 +146,12 @@ typedef struct {
   int32_t window;          /* steps per window; 0 = default (128); >= K = full trellis    */
   int32_t guard;           /* warm-up steps on each side; < 0 = default (96); multiple of 8 */
   uint32_t memory;         /* TC_MEM_HOST, TC_MEM_DEVICE or TC_MEM_HOST_ASYNC              */
-  uint32_t schedule;       /* TC_SCHEDULE_PLAIN or TC_SCHEDULE_PERSISTENT                 */
+  uint32_t schedule;       /* TC_SCHEDULE_PLAIN, TC_SCHEDULE_PERSISTENT or TC_SCHEDULE_AUTO */
   const float* scales;     /* host array, 2 per iteration (upper, lower); NULL = 1.0     */
-  uint32_t graph;          /* TC_MEM_DEVICE only: capture this request's launch sequence in a
-                              CUDA graph the first time and replay it when the same shapes,
-                              buffers and options come again (16 graphs kept per decoder);
+  uint32_t graph;          /* TC_MEM_DEVICE only (tc_decode, tc_decode_transport_blocks):
+                              capture this request's launch sequence in a CUDA graph the first
+                              time and replay it when the same shapes, buffers and options come
+                              again (16 graphs kept per decoder);
                               needs a created stream (the legacy default stream cannot be
                               captured: TC_ERR_INVALID_ARGUMENT)                          */
   void* stream;            /* cudaStream_t; TC_MEM_DEVICE: used as given (NULL = the legacy
@@ -257,7 +258,10 @@ TC_API int tc_derate_combine_llr_device(tc_decoder* dec, size_t n_tx, const tc_r
  * opts->memory like the rate-matched LLRs.  TC_MEM_HOST_ASYNC (new): host pointers; the call
  * is enqueued on one of the decoder's three worker workspaces and returns, so that one call's
  * copies overlap earlier calls' decoding; results are valid, and the inputs may be reused,
- * after tc_decoder_sync (pinned buffers for the overlap). */
+ * after tc_decoder_sync (pinned buffers for the overlap).  TC_SCHEDULE_AUTO takes the schedule
+ * and window that tc_autotune found for the code blocks' decode request (same signature); with
+ * TC_MEM_DEVICE and opts->graph the whole chain -- de-rate matching, decoding, finish -- is
+ * captured in one CUDA graph per request key (descriptors, buffers, options) and replayed. */
 typedef struct {
   int64_t tbs;         /* transport block size, without CRC24A */
   int32_t first_cb;

@@ -148,3 +148,59 @@ def test_transport_blocks_async_host_calls(tc, schedule):
         assert np.array_equal(tb_ok.numpy().astype(bool), np.asarray(ref_tb, bool))
         assert np.array_equal(cb_ok.numpy().astype(bool), np.asarray(ref_cb, bool))
         assert np.array_equal(it.numpy().astype(np.uint32), np.asarray(ref_it, np.uint32))
+
+
+def test_transport_block_graph_with_autotuned_schedule(tc, decoder):
+    """Config-3 style transport blocks on device buffers with SCHEDULE_AUTO (after tc_autotune
+    on the same code blocks) and graph replay: the first call captures de-rate matching,
+    decoding and the finish kernel, later calls replay them; every call equals the eager
+    (uncaptured) decode of the same inputs, including after new LLRs are written into the same
+    input buffer."""
+    import torch
+    from turbo_cpp_b200.workloads import config3_transport_blocks
+
+    tbs, blocks, e_llr, _, _ = config3_transport_blocks(24, seed=5)
+    tbs2, blocks2, e_llr2, _, _ = config3_transport_blocks(24, seed=5, llr_seed=77)
+    assert tbs2 == tbs and blocks2 == blocks and not np.array_equal(e_llr, e_llr2)
+    arr, e_len, llr_len = tc.Decoder.rm_blocks(blocks)
+    tba, nbits = tc.Decoder.tb_descriptors(tbs)
+    n_tb, n_cb = len(tbs), len(blocks)
+    stream = torch.cuda.Stream()
+    x = torch.from_numpy(np.ascontiguousarray(e_llr, np.float32)).cuda()
+
+    def run(opts):
+        bits = torch.zeros(nbits, dtype=torch.uint8, device="cuda")
+        tb_ok = torch.zeros(n_tb, dtype=torch.uint8, device="cuda")
+        cb_ok = torch.zeros(n_cb, dtype=torch.uint8, device="cuda")
+        it = torch.zeros(n_cb, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        decoder.decode_tbs_device(tba, n_tb, arr, n_cb, e_len, x.data_ptr(), nbits,
+                                  bits.data_ptr(), tb_ok.data_ptr(), cb_ok.data_ptr(),
+                                  it.data_ptr(), options=opts, stream=stream.cuda_stream)
+        stream.synchronize()
+        return [t.cpu().numpy() for t in (bits, tb_ok, cb_ok, it)]
+
+    # the decode request the chain makes: its de-rate-matched blocks, tuned once
+    d012 = torch.zeros(llr_len, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    decoder.derate_device(blocks, x.data_ptr(), e_len, d012.data_ptr(), llr_len,
+                          stream=stream.cuda_stream)
+    cbs, _, post_len = tc.Decoder.layout([b[0] for b in blocks], [b[1] for b in blocks])
+    post = torch.empty(post_len, dtype=torch.float32, device="cuda")
+    tuned = decoder.autotune(cbs, n_cb, d012.data_ptr(), llr_len, post.data_ptr(), post_len,
+                             tc.DecodeOptions(8, True), stream.cuda_stream)
+    stream.synchronize()
+    sched = tc.SCHEDULE_PERSISTENT if tuned["schedule"] == 1 else tc.SCHEDULE_PLAIN
+    eager = run(tc.DecodeOptions(8, True, tuned["window"], -1, sched))
+    auto_graph = tc.DecodeOptions(8, True, 0, -1, tc.SCHEDULE_AUTO, graph=True)
+    for _ in range(3):  # capture, then replays
+        got = run(auto_graph)
+        for a, b in zip(got, eager):
+            assert np.array_equal(a, b)
+    # new LLRs in the same buffer: the replayed graph decodes them
+    x.copy_(torch.from_numpy(np.ascontiguousarray(e_llr2, np.float32)))
+    eager2 = run(tc.DecodeOptions(8, True, tuned["window"], -1, sched))
+    got2 = run(auto_graph)
+    for a, b in zip(got2, eager2):
+        assert np.array_equal(a, b)
+    assert not np.array_equal(eager2[3], eager[3]) or not np.array_equal(eager2[0], eager[0])

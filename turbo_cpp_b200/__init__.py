@@ -676,6 +676,20 @@ class Decoder:
               C.addressof(arr), int(e_len), e_llr_ptr, int(bits_len), bits_ptr,
               tb_ok_ptr or None, cb_ok_ptr or None, iters_ptr or None, None, C.addressof(opt))
 
+    def decode_tbs_device(self, tba, n_tb: int, arr, n_cb: int, e_len: int, e_llr_ptr: int,
+                          bits_len: int, bits_ptr: int, tb_ok_ptr: int = 0, cb_ok_ptr: int = 0,
+                          iters_ptr: int = 0, options: Optional[DecodeOptions] = None,
+                          stream: int = 0) -> None:
+        """tc_decode_transport_blocks with TC_MEM_DEVICE: device pointers, descriptors from
+        tb_descriptors() and rm_blocks(), ordered on `stream`; returns once enqueued.  With
+        options.graph the chain is captured once per request key and replayed (needs a created
+        stream); SCHEDULE_AUTO applies the autotuning table."""
+        o = options or DecodeOptions()
+        opt, _keep = self._opts(o, MEM_DEVICE, stream)
+        _call("tc_decode_transport_blocks", self._h, int(n_tb), C.addressof(tba), int(n_cb),
+              C.addressof(arr), int(e_len), e_llr_ptr, int(bits_len), bits_ptr,
+              tb_ok_ptr or None, cb_ok_ptr or None, iters_ptr or None, None, C.addressof(opt))
+
     def decode_tbs(self, tbs, blocks, e_llr, options: Optional[DecodeOptions] = None,
                    want_posterior: bool = False):
         """Many transport blocks through the device chain (host arrays): tbs = list of

@@ -499,6 +499,8 @@ int tc_decode_transport_blocks(tc_decoder* dec, size_t n_tb, const tc_transport_
     q.decode.window = o.window;
     q.decode.guard = o.guard;
     q.decode.persistent = o.schedule == TC_SCHEDULE_PERSISTENT;
+    q.decode.auto_schedule = o.schedule == TC_SCHEDULE_AUTO;
+    q.decode.graph = o.graph != 0;  // honoured with TC_MEM_DEVICE
     q.decode.scales = o.scales;
     q.decode.std3gpp = convention_of(static_cast<int>(o.convention)) == tcb::Convention::Std3gpp;
     dec->impl.decode_transport_blocks(q);

@@ -322,7 +322,6 @@ void Decoder::transport_blocks(const TbRequest& q, bool wait) {
     if (tbs[t].tbs + 24 > static_cast<int64_t>(xpow_a.bytes / 4))
       throw CapacityExceeded("transport block larger than 104424 bits");
   // ---- de-rate matching, decoding, transport-block finish ----
-  derate_device(q.n_cb, rm.data(), e_llr, q.e_len, d012, static_cast<size_t>(llr_len), st);
   DecodeRequest rq = q.decode;
   rq.n_cb = q.n_cb;
   rq.cbs = cbs.data();
@@ -335,16 +334,44 @@ void Decoder::transport_blocks(const TbRequest& q, bool wait) {
   rq.device_memory = true;
   rq.stream = st;
   rq.graph = false;
-  if (rq.persistent) decode_persistent(rq); else decode_plain(rq);
-  // decode_* chained its own completion event; the finish kernel follows on the same stream
-  upload(dtb, tbs.data(), q.n_tb * sizeof(DevTb), st);
-  tb_finish_kernel<<<static_cast<unsigned>((q.n_tb * 32 + 255) / 256), 256, 0, st>>>(
-      dtb, static_cast<int>(q.n_tb), static_cast<const DevCb*>(d_cbs_.ptr), post,
-      static_cast<const uint32_t*>(xpow_a.ptr),
-      static_cast<const uint32_t*>(std3gpp ? d_xpow_std_.ptr : d_xpow_.ptr), bits,
-      tb_ok, cb_ok);
-  check(cudaGetLastError(), "finish launch");
-  timing_.launches += 1;
+  if (rq.auto_schedule) rq = resolve_locked(rq);  // the tuning table's schedule and window
+  auto body = [&] {
+    derate_device(q.n_cb, rm.data(), e_llr, q.e_len, d012, static_cast<size_t>(llr_len), st);
+    if (rq.persistent) decode_persistent(rq); else decode_plain(rq);
+    // decode_* chained its own completion event; the finish kernel follows on the same stream
+    upload(dtb, tbs.data(), q.n_tb * sizeof(DevTb), st);
+    tb_finish_kernel<<<static_cast<unsigned>((q.n_tb * 32 + 255) / 256), 256, 0, st>>>(
+        dtb, static_cast<int>(q.n_tb), static_cast<const DevCb*>(d_cbs_.ptr), post,
+        static_cast<const uint32_t*>(xpow_a.ptr),
+        static_cast<const uint32_t*>(std3gpp ? d_xpow_std_.ptr : d_xpow_.ptr), bits, tb_ok, cb_ok);
+    check(cudaGetLastError(), "finish launch");
+    timing_.launches += 1;
+    if (q.device_memory && q.posterior)
+      check(cudaMemcpyAsync(q.posterior, post, static_cast<size_t>(post_len) * 4,
+                            cudaMemcpyDeviceToDevice, st), "copy");
+  };
+  if (q.decode.graph && q.device_memory) {
+    // capture once per key (every descriptor, buffer address and option baked into the
+    // launches), then replay: one graph launch per call
+    std::string key = "tb";
+    auto put = [&key](const void* p, size_t n) { key.append(static_cast<const char*>(p), n); };
+    const uintptr_t ptrs[6] = {reinterpret_cast<uintptr_t>(e_llr), reinterpret_cast<uintptr_t>(bits),
+                               reinterpret_cast<uintptr_t>(tb_ok), reinterpret_cast<uintptr_t>(cb_ok),
+                               reinterpret_cast<uintptr_t>(iters),
+                               reinterpret_cast<uintptr_t>(q.posterior)};
+    const int64_t opts[9] = {static_cast<int64_t>(q.n_tb), static_cast<int64_t>(q.n_cb),
+                             static_cast<int64_t>(q.e_len), static_cast<int64_t>(q.bits_len),
+                             rq.max_iterations, rq.early_stop, rq.window, rq.guard,
+                             (rq.std3gpp ? 4 : 0) | (rq.persistent ? 2 : 0) | (rq.smem_checkpoints ? 1 : 0)};
+    put(ptrs, sizeof ptrs);
+    put(opts, sizeof opts);
+    put(rm.data(), q.n_cb * sizeof(RmBlockDesc));
+    put(tbs.data(), q.n_tb * sizeof(DevTb));
+    if (rq.scales) put(rq.scales, 2 * rq.max_iterations * sizeof(float));
+    launch_graph(graph_for(key, st, body), st);
+    return;
+  }
+  body();
   if (!q.device_memory) {
     check(cudaMemcpyAsync(q.bits, bits, static_cast<size_t>(bits_len), cudaMemcpyDeviceToHost, st),
           "copy bits out");
@@ -355,9 +382,6 @@ void Decoder::transport_blocks(const TbRequest& q, bool wait) {
     if (q.posterior)
       check(cudaMemcpyAsync(q.posterior, post, static_cast<size_t>(post_len) * 4,
                             cudaMemcpyDeviceToHost, st), "copy");
-  } else if (q.posterior) {
-    check(cudaMemcpyAsync(q.posterior, post, static_cast<size_t>(post_len) * 4,
-                          cudaMemcpyDeviceToDevice, st), "copy");
   }
   mark_done(st);
   if (!q.device_memory && wait) {

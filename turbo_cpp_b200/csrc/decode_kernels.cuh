@@ -14,7 +14,7 @@ namespace tcb {
 namespace {
 
 constexpr int kThreads = 64;  // threads (windows) per block of the plain SISO kernel
-constexpr int kMinBlocks = 10;  // 20 warps per SM: at most 96 registers per thread
+constexpr int kMinBlocks = 8;  // 16 warps per SM: at most 128 registers per thread
 
 // KIND: 0 = upper SISO, 1 = lower SISO, 2 = lower SISO that also writes the posterior;
 // STD: the TS 36.212 code instead of the reference's
@@ -115,7 +115,7 @@ __global__ void finish_kernel(int n_cb, const uint8_t* __restrict__ done, uint8_
 // kernel always terminates.  Blocks whose CRC24B passes are skipped by every later item.
 // ------------------------------------------------------------------------------------------
 constexpr int kPersistThreads = 64;
-constexpr int kPersistMinBlocks = 8;
+constexpr int kPersistMinBlocks = 6;  // 12 warps per SM: at most 168 registers per thread
 constexpr int kMaxIterations = 64;
 constexpr uint64_t kWaitLimitNs = 1000000000ull;  // one second
 

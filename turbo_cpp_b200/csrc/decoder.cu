@@ -7,6 +7,8 @@
 // 1719-1899), batched over code blocks and correct for every K.
 #include <cuda_runtime.h>
 
+#include <functional>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -308,10 +310,14 @@ std::string Decoder::signature(const DecodeRequest& rq) {
 }
 
 DecodeRequest Decoder::resolve(const DecodeRequest& rq) {
+  std::lock_guard<std::mutex> lock(mu_);
+  return resolve_locked(rq);
+}
+
+DecodeRequest Decoder::resolve_locked(const DecodeRequest& rq) const {
   DecodeRequest r = rq;
   r.auto_schedule = false;
   const std::string sig = signature(rq);
-  std::lock_guard<std::mutex> lock(mu_);
   for (const auto& kv : tuning_)
     if (kv.first == sig) {
       r.persistent = kv.second.persistent;
@@ -424,13 +430,84 @@ void Decoder::load_tuning(const std::string& path) {
 
 // Capture-once / replay: the key covers everything baked into the captured launches (block
 // descriptors, buffer addresses, options, scales); a workspace reallocation invalidates it.
+// Called with mu_ held.  `body` enqueues the launches on `st`; on a miss it runs once eagerly
+// (sizing the workspace and the descriptor uploads, so that capturing allocates nothing) and
+// once under capture.  Returns the entry to launch.
+Decoder::GraphEntry* Decoder::graph_for(const std::string& key, void* stream,
+                                        const std::function<void()>& body) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (st == nullptr || st == cudaStreamLegacy)
+    throw InvalidArgument("graph: the legacy default stream cannot be captured; pass a created stream");
+  for (auto it = graphs_.begin(); it != graphs_.end(); ++it)
+    if (it->key == key) {
+      if (it->generation == generation_) {
+        graphs_.splice(graphs_.begin(), graphs_, it);  // most recently used first
+        return &graphs_.front();
+      }
+      drop_graph(*it);
+      graphs_.erase(it);
+      break;
+    }
+  upload_bytes_ = 0;
+  body();  // the dry run
+  graphs_.emplace_front();
+  GraphEntry& e = graphs_.front();
+  e.key = key;
+  e.arena_bytes = upload_bytes_;
+  check(cudaMallocHost(&e.arena, std::max<size_t>(e.arena_bytes, 256)), "cudaMallocHost");
+  const uint64_t launches_before = timing_.launches;
+  const bool timing_was = timing_on_;
+  timing_on_ = false;
+  capturing_ = &e;
+  cudaGraph_t g = nullptr;
+  // any failure from here on removes the half-made entry, so that no later call replays it
+  cudaGraphExec_t exec = nullptr;
+  try {
+    check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    try {
+      body();
+    } catch (...) {
+      cudaStreamEndCapture(st, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    check(cudaStreamEndCapture(st, &g), "cudaStreamEndCapture");
+    const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    check(ie, "cudaGraphInstantiate");
+  } catch (...) {
+    capturing_ = nullptr;
+    timing_on_ = timing_was;
+    timing_.launches = launches_before;
+    drop_graph(e);
+    graphs_.pop_front();
+    throw;
+  }
+  capturing_ = nullptr;
+  timing_on_ = timing_was;
+  e.exec = exec;
+  e.generation = generation_;
+  e.launches = timing_.launches - launches_before;
+  timing_.launches = launches_before;
+  while (graphs_.size() > 16) {  // keep the most recent 16
+    drop_graph(graphs_.back());
+    graphs_.pop_back();
+  }
+  return &graphs_.front();
+}
+
+void Decoder::launch_graph(GraphEntry* e, void* stream) {
+  order_after_previous(stream);
+  check(cudaGraphLaunch(static_cast<cudaGraphExec_t>(e->exec), static_cast<cudaStream_t>(stream)),
+        "cudaGraphLaunch");
+  mark_done(stream);
+  timing_.launches += e->launches;
+}
+
 void Decoder::decode_graph(const DecodeRequest& rq) {
   std::lock_guard<std::mutex> lock(mu_);
   check(cudaSetDevice(device_), "cudaSetDevice");
-  cudaStream_t st = static_cast<cudaStream_t>(rq.stream);
-  if (st == nullptr || st == cudaStreamLegacy)
-    throw InvalidArgument("graph: the legacy default stream cannot be captured; pass a created stream");
-  std::string key;
+  std::string key = "cb";
   auto put = [&key](const void* p, size_t n) { key.append(static_cast<const char*>(p), n); };
   const uintptr_t ptrs[4] = {reinterpret_cast<uintptr_t>(rq.llr),
                              reinterpret_cast<uintptr_t>(rq.posterior),
@@ -444,76 +521,12 @@ void Decoder::decode_graph(const DecodeRequest& rq) {
   put(opts, sizeof opts);
   put(rq.cbs, rq.n_cb * sizeof(CodeBlockDesc));
   if (rq.scales) put(rq.scales, 2 * rq.max_iterations * sizeof(float));
-  GraphEntry* hit = nullptr;
-  for (auto it = graphs_.begin(); it != graphs_.end(); ++it)
-    if (it->key == key) {
-      if (it->generation == generation_) {
-        graphs_.splice(graphs_.begin(), graphs_, it);  // most recently used first
-        hit = &graphs_.front();
-      } else {
-        drop_graph(*it);
-        graphs_.erase(it);
-      }
-      break;
-    }
-  if (hit == nullptr) {
-    // size the workspace and the descriptor uploads first (outside the capture), so that
-    // capturing allocates nothing
-    upload_bytes_ = 0;
-    {
-      DecodeRequest dry = rq;
-      dry.graph = false;
-      if (rq.persistent) decode_persistent(dry); else decode_plain(dry);
-    }
-    graphs_.emplace_front();
-    GraphEntry& e = graphs_.front();
-    e.key = key;
-    e.arena_bytes = upload_bytes_;
-    check(cudaMallocHost(&e.arena, std::max<size_t>(e.arena_bytes, 256)), "cudaMallocHost");
-    const uint64_t launches_before = timing_.launches;
-    const bool timing_was = timing_on_;
-    timing_on_ = false;
-    capturing_ = &e;
-    cudaGraph_t g = nullptr;
-    // any failure from here on removes the half-made entry, so that no later call replays it
-    cudaGraphExec_t exec = nullptr;
-    try {
-      check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
-      try {
-        if (rq.persistent) decode_persistent(rq); else decode_plain(rq);
-      } catch (...) {
-        cudaStreamEndCapture(st, &g);
-        if (g) cudaGraphDestroy(g);
-        throw;
-      }
-      check(cudaStreamEndCapture(st, &g), "cudaStreamEndCapture");
-      const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
-      cudaGraphDestroy(g);
-      check(ie, "cudaGraphInstantiate");
-    } catch (...) {
-      capturing_ = nullptr;
-      timing_on_ = timing_was;
-      timing_.launches = launches_before;
-      drop_graph(e);
-      graphs_.pop_front();
-      throw;
-    }
-    capturing_ = nullptr;
-    timing_on_ = timing_was;
-    e.exec = exec;
-    e.generation = generation_;
-    e.launches = timing_.launches - launches_before;
-    timing_.launches = launches_before;
-    while (graphs_.size() > 16) {  // keep the most recent 16
-      drop_graph(graphs_.back());
-      graphs_.pop_back();
-    }
-    hit = &e;
-  }
-  order_after_previous(st);
-  check(cudaGraphLaunch(static_cast<cudaGraphExec_t>(hit->exec), st), "cudaGraphLaunch");
-  mark_done(st);
-  timing_.launches += hit->launches;
+  DecodeRequest eager = rq;
+  eager.graph = false;
+  GraphEntry* e = graph_for(key, rq.stream, [&] {
+    if (eager.persistent) decode_persistent(eager); else decode_plain(eager);
+  });
+  launch_graph(e, rq.stream);
 }
 
 namespace {

@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <functional>
 #include <list>
 #include <memory>
 #include <mutex>
@@ -211,6 +212,10 @@ class Decoder {
   std::list<GraphEntry> graphs_;
   std::vector<std::pair<std::string, TuneChoice>> tuning_;
   DecodeRequest resolve(const DecodeRequest& rq);  // applies the tuning table to an auto request
+  DecodeRequest resolve_locked(const DecodeRequest& rq) const;  // the same, mu_ already held
+  // the cached graph of `key`, captured from `body` on a miss (mu_ held), and its launch
+  GraphEntry* graph_for(const std::string& key, void* stream, const std::function<void()>& body);
+  void launch_graph(GraphEntry* e, void* stream);
   GraphEntry* capturing_ = nullptr;       // entry being captured (uploads go to its staging)
   uint64_t generation_ = 0;               // bumped whenever a workspace buffer moves
   size_t upload_bytes_ = 0;               // descriptor bytes uploaded (sizes a graph's arena)

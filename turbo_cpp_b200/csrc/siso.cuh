@@ -167,7 +167,9 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
   float sa[4], a[4], b[4];
 
   // ---- forward: warm-up from a_lo, then a checkpoint every 4 steps over [lo, hi) ----
-  float al[8];
+  // Metrics in (m, s) form (trellis.cuh); seeds and checkpoints are log values.
+  float al[8], as[8];
+  ms_ones(as);
   int a_lo = lo - G;
   if (a_lo <= 0) {
     a_lo = 0;
@@ -181,14 +183,22 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
     for (int q = a_lo; q < hi; q += 8) {
       Raw8 nxt = cur;
       if (q + 8 < hi) nxt = load_raw8<COHERENT>(sys, apr, par, q + 8);
-      if (q >= lo) ck.store((q - lo) / S, al);
+      float v[8];
+      if (q >= lo) {
+        ms_to_log(al, as, v);
+        ck.store((q - lo) / S, v);
+      }
       scale4(cur.lo, sa, a, b);
 #pragma unroll
-      for (int t = 0; t < 4; ++t) alpha_step<STD>(al, a[t], b[t]);
-      if (q >= lo) ck.store((q - lo) / S + 1, al);
+      for (int t = 0; t < 4; ++t) alpha_step_ms<STD>(al, as, a[t], b[t]);
+      if (q >= lo) {
+        ms_to_log(al, as, v);
+        ck.store((q - lo) / S + 1, v);
+      }
       scale4(cur.hi, sa, a, b);
 #pragma unroll
-      for (int t = 0; t < 4; ++t) alpha_step<STD>(al, a[t], b[t]);
+      for (int t = 0; t < 4; ++t) alpha_step_ms<STD>(al, as, a[t], b[t]);
+      ms_renorm(al, as);
       cur = nxt;
     }
   }
@@ -196,8 +206,7 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
   if (w + 1 < cb.nwin && hi - G > 0) {
     float r[8];
     if (G == 0) {
-#pragma unroll
-      for (int s = 0; s < 8; ++s) r[s] = al[s];
+      ms_to_log(al, as, r);
     } else {
       ck.load((hi - G - lo) / S, r);
     }
@@ -207,7 +216,8 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
   }
 
   // ---- backward: warm-up from b_hi down to hi ----
-  float be[8];
+  float be[8], bs[8];
+  ms_ones(bs);
   int b_hi = hi + G;
   if (b_hi >= K) {
     b_hi = K;
@@ -225,18 +235,21 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
       if (q - 8 >= hi) nxt = load_raw8<COHERENT>(sys, apr, par, q - 8);
       scale4(cur.hi, sa, a, b);
 #pragma unroll
-      for (int t = 3; t >= 0; --t) beta_step<STD>(be, a[t], b[t]);
+      for (int t = 3; t >= 0; --t) beta_step_ms<STD>(be, bs, a[t], b[t]);
       scale4(cur.lo, sa, a, b);
 #pragma unroll
-      for (int t = 3; t >= 0; --t) beta_step<STD>(be, a[t], b[t]);
+      for (int t = 3; t >= 0; --t) beta_step_ms<STD>(be, bs, a[t], b[t]);
+      ms_renorm(be, bs);
       cur = nxt;
     }
   }
   const bool rec_beta = (w > 0) && (lo + G <= hi);
   float4* bseed = rec_beta ? reinterpret_cast<float4*>(io.seed_out + 16 * (g - 1) + 8) : nullptr;
   if (rec_beta && lo + G == hi) {
-    bseed[0] = make_float4(be[0], be[1], be[2], be[3]);
-    bseed[1] = make_float4(be[4], be[5], be[6], be[7]);
+    float r[8];
+    ms_to_log(be, bs, r);
+    bseed[0] = make_float4(r[0], r[1], r[2], r[3]);
+    bseed[1] = make_float4(r[4], r[5], r[6], r[7]);
   }
 
   // ---- per 4-step sub-window (last to first): recompute alpha, then beta + extrinsic.  The
@@ -256,9 +269,12 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
     const int base = lo + j * S;
     const Raw4 r = r_n;
     const uint2 iv = i_n;
-    float Al[S][8];
+    float Al[S][8], As[S][8];
 #pragma unroll
-    for (int s = 0; s < 8; ++s) Al[0][s] = c_n[s];
+    for (int k = 0; k < 8; ++k) {
+      Al[0][k] = c_n[k];
+      As[0][k] = 1.0f;
+    }
     if (j > 0) {
       r_n = load_raw4<COHERENT>(sys, apr, par, base - S);
       i_n = __ldg(reinterpret_cast<const uint2*>(pt + base - S));
@@ -269,22 +285,28 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
 #pragma unroll
     for (int t = 0; t + 1 < S; ++t) {
 #pragma unroll
-      for (int s = 0; s < 8; ++s) Al[t + 1][s] = Al[t][s];
-      alpha_step<STD>(Al[t + 1], A_[t], B_[t]);
+      for (int k = 0; k < 8; ++k) {
+        Al[t + 1][k] = Al[t][k];
+        As[t + 1][k] = As[t][k];
+      }
+      alpha_step_ms<STD>(Al[t + 1], As[t + 1], A_[t], B_[t]);
     }
     const uint32_t w2[2] = {iv.x, iv.y};
 #pragma unroll
     for (int t = S - 1; t >= 0; --t) {
-      const float e = io.scale * (kLn2 * extrinsic2<STD>(Al[t], be, B_[t]));
+      const float e = io.scale * (kLn2 * extrinsic_ms<STD>(Al[t], As[t], be, bs, B_[t]));
       const int n = static_cast<int>((w2[t >> 1] >> (16 * (t & 1))) & 0xffffu);
       io.ext[cb.work + n] = e;
       if (POST) io.post[cb.out + n] = SA[t] + e;
-      beta_step<STD>(be, A_[t], B_[t]);
+      beta_step_ms<STD>(be, bs, A_[t], B_[t]);
       if (rec_beta && base + t == lo + G) {
-        bseed[0] = make_float4(be[0], be[1], be[2], be[3]);
-        bseed[1] = make_float4(be[4], be[5], be[6], be[7]);
+        float rr[8];
+        ms_to_log(be, bs, rr);
+        bseed[0] = make_float4(rr[0], rr[1], rr[2], rr[3]);
+        bseed[1] = make_float4(rr[4], rr[5], rr[6], rr[7]);
       }
     }
+    ms_renorm(be, bs);
   }
 }
 

@@ -160,4 +160,113 @@ __device__ __forceinline__ void alpha_start(float (&al)[8]) {
   for (int s = 1; s < 8; ++s) al[s] = kNegBig;
 }
 
+// ------------------------------------------------------------------------------------------
+// Deferred-logarithm form of the recursions.  A state metric is a pair (m, s) standing for the
+// base-2 log value m + log2(s), s >= 1.  The Jacobian logarithm of two branches x = (mx, sx),
+// y = (my, sy) is then exact without a logarithm:
+//     log2(sx 2^mx + sy 2^my) = max(mx, my) + log2(s_hi + s_lo 2^-|mx - my|),
+// where s_hi belongs to the larger m and s_lo to the other: one ex2 and one FMA per state and
+// step instead of an ex2 and an lg2.  s grows by at most a factor of two per step and is folded
+// back into m (its binary exponent, integer operations only) every few steps; the log values
+// m + lg2(s) are formed only where metrics leave the thread (seeds, checkpoints).  The values
+// are the same Jacobian logarithms as max_star's, up to float rounding.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void ms_join(float x, float y, float sx, float sy, float& m, float& s) {
+  const float d = x - y;
+  const float t = ex2(-fabsf(d));
+  const bool c = d >= 0.0f;
+  s = fmaf(c ? sy : sx, t, c ? sx : sy);
+  m = fmaxf(x, y);
+}
+
+// alpha_{t+1} from alpha_t in (m, s) form; m normalised so that state 0's m is 0.
+template <bool STD = false>
+__device__ __forceinline__ void alpha_step_ms(float (&m)[8], float (&s)[8], float a, float b) {
+  const float g0 = a + b, g1 = a - b;
+  float mn[8], sn[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) {
+    const int p0 = 2 * (n & 3);
+    ms_join(m[p0] + branch(pred_input<STD>(n, 0), pred_parity(n, 0), g0, g1),
+            m[p0 + 1] + branch(pred_input<STD>(n, 1), pred_parity(n, 1), g0, g1), s[p0],
+            s[p0 + 1], mn[n], sn[n]);
+  }
+  const float r = mn[0];
+  m[0] = 0.0f;
+#pragma unroll
+  for (int k = 1; k < 8; ++k) m[k] = mn[k] - r;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s[k] = sn[k];
+}
+
+// beta_t from beta_{t+1} in (m, s) form; m normalised so that state 0's m is 0.
+template <bool STD = false>
+__device__ __forceinline__ void beta_step_ms(float (&m)[8], float (&s)[8], float a, float b) {
+  const float g0 = a + b, g1 = a - b;
+  float mn[8], sn[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int n0 = next_state<STD>(k, 0), n1 = next_state<STD>(k, 1);
+    ms_join(m[n0] + branch(0, parity<STD>(k, 0), g0, g1),
+            m[n1] + branch(1, parity<STD>(k, 1), g0, g1), s[n0], s[n1], mn[k], sn[k]);
+  }
+  const float r = mn[0];
+  m[0] = 0.0f;
+#pragma unroll
+  for (int k = 1; k < 8; ++k) m[k] = mn[k] - r;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s[k] = sn[k];
+}
+
+// Folds the binary exponent of each s (s >= 1) into its m, leaving s in [1, 2).
+__device__ __forceinline__ void ms_renorm(float (&m)[8], float (&s)[8]) {
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int bits = __float_as_int(s[k]);
+    const int e = (bits >> 23) - 127;
+    s[k] = __int_as_float(bits - (e << 23));
+    m[k] += static_cast<float>(e);
+  }
+}
+
+// (m, s) -> log values m + lg2(s), normalised so that state 0 is 0.
+__device__ __forceinline__ void ms_to_log(const float (&m)[8], const float (&s)[8], float (&v)[8]) {
+  float r[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) r[k] = m[k] + lg2(s[k]);
+  v[0] = 0.0f;
+#pragma unroll
+  for (int k = 1; k < 8; ++k) v[k] = r[k] - r[0];
+}
+
+__device__ __forceinline__ void ms_ones(float (&s)[8]) {
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s[k] = 1.0f;
+}
+
+// Extrinsic LLR (base 2) of one step from alpha_t and beta_{t+1} in (m, s) form: the same
+// two 8-way log-sums as extrinsic2, each max + lg2(sum s_a s_b 2^(m - max)).
+template <bool STD = false>
+__device__ __forceinline__ float extrinsic_ms(const float (&ma)[8], const float (&sa)[8],
+                                              const float (&mb)[8], const float (&sb)[8],
+                                              float b) {
+  float m0[8], m1[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    m0[k] = ma[k] + mb[next_state<STD>(k, 0)] + (parity<STD>(k, 0) ? b : -b);
+    m1[k] = ma[k] + mb[next_state<STD>(k, 1)] + (parity<STD>(k, 1) ? b : -b);
+  }
+  const float x0 = fmaxf(fmaxf(fmaxf(m0[0], m0[1]), fmaxf(m0[2], m0[3])),
+                         fmaxf(fmaxf(m0[4], m0[5]), fmaxf(m0[6], m0[7])));
+  const float x1 = fmaxf(fmaxf(fmaxf(m1[0], m1[1]), fmaxf(m1[2], m1[3])),
+                         fmaxf(fmaxf(m1[4], m1[5]), fmaxf(m1[6], m1[7])));
+  float s0 = 0.0f, s1 = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    s0 = fmaf(sa[k] * sb[next_state<STD>(k, 0)], ex2(m0[k] - x0), s0);
+    s1 = fmaf(sa[k] * sb[next_state<STD>(k, 1)], ex2(m1[k] - x1), s1);
+  }
+  return (x1 - x0) + (lg2(s1) - lg2(s0));
+}
+
 }  // namespace tcb
