@@ -150,7 +150,7 @@ struct AdjIo {
   float* guard_g;         // [launch window][4][guard]: alpha warm-up sa, par; beta warm-up sa, par
   float* tail_g;          // [launch window][8]: d/d ts[0..2], d/d tp[0..2] (tail-started windows)
   float* scale_part;      // [launch window]: sum of ge * x over the window
-  float4* ckpt;           // [launch window][2 * ckpt_slots]: alpha then beta checkpoints
+  float4* ckpt;           // alpha then beta checkpoints: 2 * ckpt_slots planes of n_win float4 each
   int ckpt_slots;         // checkpoints of each kind per window
   float scale;
   int guard;
@@ -199,8 +199,9 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
   const float* sys = LOWER ? io.sys_i + cb.work : d0;
   const float* par = d0 + (LOWER ? 2 : 1) * (K + 4);
   const float* apr = io.apr + cb.work;
-  const CkptGlobal cka{io.ckpt + static_cast<int64_t>(4) * io.ckpt_slots * g};
-  const CkptGlobal ckb{io.ckpt + static_cast<int64_t>(4) * io.ckpt_slots * g + 2 * io.ckpt_slots};
+  // alpha then beta checkpoints, each a slab of planes with the launch's windows interleaved
+  const CkptStrided cka{io.ckpt, n_win, g};
+  const CkptStrided ckb{io.ckpt + static_cast<int64_t>(2) * io.ckpt_slots * n_win, n_win, g};
   float sa[4], a[4], b[4];
   float* ag = io.guard_g + static_cast<int64_t>(4 * g) * G;
   const float xs = kLn2 * io.scale;  // d e / d(base-2 extrinsic)

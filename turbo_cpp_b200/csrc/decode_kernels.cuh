@@ -33,8 +33,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) siso_plain_kernel(const 
   const DevCb cb = cbs[c];
   const int w = g - cb.win0;
   if (GLOBAL_CKPT) {
-    CkptGlobal ck{ckpt_global + static_cast<int64_t>(2) * ckpt_per_thread * g};
-    siso_window<S, KIND != 0, KIND == 2, CkptGlobal, false, STD>(cb, w, g, io, ck);
+    // checkpoint slab: ckpt_per_thread planes of n_win float4 pairs (windows interleaved)
+    CkptStrided ck{ckpt_global, n_win, g};
+    siso_window<S, KIND != 0, KIND == 2, CkptStrided, false, STD>(cb, w, g, io, ck);
   } else {
     CkptSmem ck{smem_ckpt, static_cast<int>(blockDim.x), static_cast<int>(threadIdx.x)};
     siso_window<S, KIND != 0, KIND == 2, CkptSmem, false, STD>(cb, w, g, io, ck);
@@ -139,6 +140,7 @@ struct PersistArgs {
   float* seed_lo[2];
   float4* ckpt;
   int ckpt_per_window;
+  int n_windows;         // windows of the launch (stride of the interleaved checkpoint slab)
   int guard;
   int max_iterations;
   int early_stop;
@@ -195,7 +197,7 @@ __global__ void __launch_bounds__(kPersistThreads, kPersistMinBlocks)
     const int w = g - cb.win0;
     const bool active = c >= 0 && __ldcg(p.done + c) == 0;
     if (__any_sync(0xffffffffu, active)) {
-      const CkptGlobal ck{p.ckpt + static_cast<int64_t>(2) * p.ckpt_per_window * (g < 0 ? 0 : g)};
+      const CkptStrided ck{p.ckpt, p.n_windows, g < 0 ? 0 : g};
       const bool post_now = p.early_stop || it + 1 == p.max_iterations;
       const SisoIo io =
           half == 0 ? SisoIo{p.llr, p.sys_i, p.e2, p.e1i, nullptr, p.perm, p.inv, p.seed_up[it & 1],
@@ -203,7 +205,7 @@ __global__ void __launch_bounds__(kPersistThreads, kPersistMinBlocks)
                     : SisoIo{p.llr, p.sys_i, p.e1i, p.e2, p.post, p.perm, p.inv, p.seed_lo[it & 1],
                              p.seed_lo[(it + 1) & 1], p.scale[2 * it + 1], p.guard};
       if (active)
-        siso_window_rt<kSub, CkptGlobal, true, STD>(cb, w, g, io, ck, half == 1,
+        siso_window_rt<kSub, decltype(ck), true, STD>(cb, w, g, io, ck, half == 1,
                                                     half == 1 && post_now);
       if (half == 1 && p.early_stop) {
         // CRC24B syndrome of the hard decisions (lte_turbo.cpp:792-804): each lane XORs

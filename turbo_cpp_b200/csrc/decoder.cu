@@ -867,6 +867,7 @@ void Decoder::decode_persistent(const DecodeRequest& rq) {
   a.seed_lo[1] = seeds + 3 * slab;
   a.ckpt = ckpt;
   a.ckpt_per_window = max_ckpt;
+  a.n_windows = n_win;
   a.guard = guard;
   a.max_iterations = static_cast<int>(rq.max_iterations);
   a.early_stop = rq.early_stop ? 1 : 0;

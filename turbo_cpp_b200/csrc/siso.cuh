@@ -10,8 +10,10 @@
 // (decode_siso_log_map, lte_turbo.cpp:410-486).
 //
 // Memory use per thread: the forward pass stores alpha only every S steps (checkpoints, 32 B
-// each, in shared memory or a global scratch slot); the backward pass recomputes the S alphas
-// of one sub-window into registers from its checkpoint and then runs beta + extrinsic over it.
+// each, in shared memory or global scratch with the windows of a launch interleaved); the
+// backward pass recomputes the S alphas of one sub-window into registers from its checkpoint
+// and then runs beta + extrinsic over it.  The metrics are in the deferred-log (m, s) form of
+// trellis.cuh, normalised every 4 steps.
 #pragma once
 #include <cstdint>
 
@@ -123,6 +125,23 @@ struct CkptGlobal {
   }
 };
 
+// Global scratch with the windows of a launch interleaved: checkpoint plane j holds one float4
+// pair per window, so the 32 lanes of a warp (consecutive windows) store and load 32
+// consecutive float4 -- four whole cache lines -- per instruction.
+struct CkptStrided {
+  float4* base;    // the launch's checkpoint slab
+  int64_t stride;  // windows of the launch (float4 pairs per plane)
+  int64_t g;       // this window
+  __device__ __forceinline__ void store(int j, const float (&m)[8]) const {
+    base[(2 * j) * stride + g] = make_float4(m[0], m[1], m[2], m[3]);
+    base[(2 * j + 1) * stride + g] = make_float4(m[4], m[5], m[6], m[7]);
+  }
+  __device__ __forceinline__ void load(int j, float (&m)[8]) const {
+    const float4 x = base[(2 * j) * stride + g], y = base[(2 * j + 1) * stride + g];
+    m[0] = x.x; m[1] = x.y; m[2] = x.z; m[3] = x.w; m[4] = y.x; m[5] = y.y; m[6] = y.z; m[7] = y.w;
+  }
+};
+
 // Tail LLRs in the reference's decoder mapping (lte_turbo.cpp:758-773), or (STD) in the
 // inverse of TS 36.212 5.1.3.2.2's multiplexing: upper systematic x_K..x_K+2 = d0[K], d2[K],
 // d1[K+1], parity z_K..z_K+2 = d1[K], d0[K+1], d2[K+1]; lower x' = d0[K+2], d2[K+2], d1[K+3],
@@ -190,14 +209,20 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
       }
       scale4(cur.lo, sa, a, b);
 #pragma unroll
-      for (int t = 0; t < 4; ++t) alpha_step_ms<STD>(al, as, a[t], b[t]);
+      for (int t = 0; t < 4; ++t) {
+        if (t == 3) alpha_step_ms<STD, true>(al, as, a[t], b[t]);
+        else alpha_step_ms<STD, false>(al, as, a[t], b[t]);
+      }
       if (q >= lo) {
         ms_to_log(al, as, v);
         ck.store((q - lo) / S + 1, v);
       }
       scale4(cur.hi, sa, a, b);
 #pragma unroll
-      for (int t = 0; t < 4; ++t) alpha_step_ms<STD>(al, as, a[t], b[t]);
+      for (int t = 0; t < 4; ++t) {
+        if (t == 3) alpha_step_ms<STD, true>(al, as, a[t], b[t]);
+        else alpha_step_ms<STD, false>(al, as, a[t], b[t]);
+      }
       ms_renorm(al, as);
       cur = nxt;
     }
@@ -235,10 +260,16 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
       if (q - 8 >= hi) nxt = load_raw8<COHERENT>(sys, apr, par, q - 8);
       scale4(cur.hi, sa, a, b);
 #pragma unroll
-      for (int t = 3; t >= 0; --t) beta_step_ms<STD>(be, bs, a[t], b[t]);
+      for (int t = 3; t >= 0; --t) {
+        if (t == 0) beta_step_ms<STD, true>(be, bs, a[t], b[t]);
+        else beta_step_ms<STD, false>(be, bs, a[t], b[t]);
+      }
       scale4(cur.lo, sa, a, b);
 #pragma unroll
-      for (int t = 3; t >= 0; --t) beta_step_ms<STD>(be, bs, a[t], b[t]);
+      for (int t = 3; t >= 0; --t) {
+        if (t == 0) beta_step_ms<STD, true>(be, bs, a[t], b[t]);
+        else beta_step_ms<STD, false>(be, bs, a[t], b[t]);
+      }
       ms_renorm(be, bs);
       cur = nxt;
     }
@@ -289,7 +320,7 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
         Al[t + 1][k] = Al[t][k];
         As[t + 1][k] = As[t][k];
       }
-      alpha_step_ms<STD>(Al[t + 1], As[t + 1], A_[t], B_[t]);
+      alpha_step_ms<STD, false>(Al[t + 1], As[t + 1], A_[t], B_[t]);
     }
     const uint32_t w2[2] = {iv.x, iv.y};
 #pragma unroll
@@ -298,7 +329,8 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
       const int n = static_cast<int>((w2[t >> 1] >> (16 * (t & 1))) & 0xffffu);
       io.ext[cb.work + n] = e;
       if (POST) io.post[cb.out + n] = SA[t] + e;
-      beta_step_ms<STD>(be, bs, A_[t], B_[t]);
+      if (t == 0) beta_step_ms<STD, true>(be, bs, A_[t], B_[t]);
+      else beta_step_ms<STD, false>(be, bs, A_[t], B_[t]);
       if (rec_beta && base + t == lo + G) {
         float rr[8];
         ms_to_log(be, bs, rr);

@@ -179,8 +179,9 @@ __device__ __forceinline__ void ms_join(float x, float y, float sx, float sy, fl
   m = fmaxf(x, y);
 }
 
-// alpha_{t+1} from alpha_t in (m, s) form; m normalised so that state 0's m is 0.
-template <bool STD = false>
+// alpha_{t+1} from alpha_t in (m, s) form; NORM: m normalised so that state 0's m is 0 (the
+// values are shift-invariant, so the recursions normalise only every few steps to bound m).
+template <bool STD = false, bool NORM = true>
 __device__ __forceinline__ void alpha_step_ms(float (&m)[8], float (&s)[8], float a, float b) {
   const float g0 = a + b, g1 = a - b;
   float mn[8], sn[8];
@@ -191,16 +192,15 @@ __device__ __forceinline__ void alpha_step_ms(float (&m)[8], float (&s)[8], floa
             m[p0 + 1] + branch(pred_input<STD>(n, 1), pred_parity(n, 1), g0, g1), s[p0],
             s[p0 + 1], mn[n], sn[n]);
   }
-  const float r = mn[0];
-  m[0] = 0.0f;
+  const float r = NORM ? mn[0] : 0.0f;
 #pragma unroll
-  for (int k = 1; k < 8; ++k) m[k] = mn[k] - r;
+  for (int k = 0; k < 8; ++k) m[k] = NORM ? mn[k] - r : mn[k];
 #pragma unroll
   for (int k = 0; k < 8; ++k) s[k] = sn[k];
 }
 
-// beta_t from beta_{t+1} in (m, s) form; m normalised so that state 0's m is 0.
-template <bool STD = false>
+// beta_t from beta_{t+1} in (m, s) form; NORM as for alpha_step_ms.
+template <bool STD = false, bool NORM = true>
 __device__ __forceinline__ void beta_step_ms(float (&m)[8], float (&s)[8], float a, float b) {
   const float g0 = a + b, g1 = a - b;
   float mn[8], sn[8];
@@ -210,10 +210,9 @@ __device__ __forceinline__ void beta_step_ms(float (&m)[8], float (&s)[8], float
     ms_join(m[n0] + branch(0, parity<STD>(k, 0), g0, g1),
             m[n1] + branch(1, parity<STD>(k, 1), g0, g1), s[n0], s[n1], mn[k], sn[k]);
   }
-  const float r = mn[0];
-  m[0] = 0.0f;
+  const float r = NORM ? mn[0] : 0.0f;
 #pragma unroll
-  for (int k = 1; k < 8; ++k) m[k] = mn[k] - r;
+  for (int k = 0; k < 8; ++k) m[k] = NORM ? mn[k] - r : mn[k];
 #pragma unroll
   for (int k = 0; k < 8; ++k) s[k] = sn[k];
 }
