@@ -570,7 +570,7 @@ uint64_t Adjoint::forward(const AdjointRequest& rq) {
   std3gpp_ = rq.std3gpp;
   scales_.assign(2 * I, 1.0f);
   if (rq.scales) std::copy(rq.scales, rq.scales + 2 * I, scales_.begin());
-  ckpt_fwd_ = max_window / kSub;
+  ckpt_fwd_ = max_window / kSub + 1;
   ckpt_bwd_ = (max_window + guard) / 4 + 1;
 
   DevCb* dcbs = reserve<DevCb>(d_cbs_, n);
@@ -579,7 +579,7 @@ uint64_t Adjoint::forward(const AdjointRequest& rq) {
   float* tape = reserve<float>(d_tape_, static_cast<size_t>(2 * I + 1) * work);
   const size_t slab = static_cast<size_t>(n_win) * 16;
   float* seeds = reserve<float>(d_seeds_, (2 * I + 2) * slab);
-  float4* ckpt = reserve<float4>(d_ckpt_, static_cast<size_t>(n_win) * 2 * ckpt_fwd_);
+  float4* ckpt = reserve<float4>(d_ckpt_, ckpt_slab(n_win, 2 * static_cast<size_t>(ckpt_fwd_)));
   ok(cudaMemcpyAsync(dcbs, cbs_.data(), n * sizeof(DevCb), cudaMemcpyHostToDevice, st), "copy descriptors");
   ok(cudaMemcpyAsync(dwin, wincb.data(), n_win * sizeof(int32_t), cudaMemcpyHostToDevice, st), "copy descriptors");
   ok(cudaMemsetAsync(seeds, 0, 2 * slab * sizeof(float), st), "zero seeds");
@@ -634,7 +634,7 @@ void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr
   float* part = reserve<float>(d_part_, static_cast<size_t>(2 * I) * n_win);
   float* ge2 = reserve<float>(d_ge2_, work);
   float* ga1 = reserve<float>(d_ga1_, work);
-  float4* ckpt = reserve<float4>(d_ckpt_, static_cast<size_t>(n_win) * 4 * ckpt_bwd_);
+  float4* ckpt = reserve<float4>(d_ckpt_, ckpt_slab(n_win, 4 * static_cast<size_t>(ckpt_bwd_)));
   const DevCb* dcbs = static_cast<const DevCb*>(d_cbs_.ptr);
   const int32_t* dwin = static_cast<const int32_t*>(d_wincb_.ptr);
   const float* sysi = static_cast<const float*>(d_sysi_.ptr);

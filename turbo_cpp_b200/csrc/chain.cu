@@ -248,6 +248,7 @@ void Decoder::decode_transport_blocks(const TbRequest& q) {
     while (workers_.size() < kAsyncWorkers) workers_.push_back(std::make_unique<Decoder>(device_));
     Decoder& w = *workers_[next_worker_];
     next_worker_ = (next_worker_ + 1) % workers_.size();
+    w.tuning_ = tuning_;  // SCHEDULE_AUTO resolves on the worker: give it this decoder's table
     TbRequest r = q;
     r.host_async = false;
     r.stream = nullptr;  // the worker's own stream

@@ -340,11 +340,12 @@ Decoder::TuneChoice Decoder::autotune(const DecodeRequest& rq_in) {
   const int guard = rq_in.guard < 0 ? kDefaultGuard : rq_in.guard;
   // Plain-schedule windows that fill whole waves: the smallest window (a multiple of 8, at
   // least the guard) whose windows over all blocks fit in j resident waves of the SISO kernel
-  // (SMs x blocks per SM x threads per block), for j = 2, 3, 4.  A launch with a partly filled
+  // (SMs x blocks per SM x threads per block), for j = 1 .. 4.  A launch with a partly filled
   // last wave idles SMs for the length of a window (measured at 4096 x K=6144: window 136 = two
-  // full waves 2606 Mbit/s, window 128 = 2.07 waves 2457 Mbit/s).
+  // full waves 2606 Mbit/s, window 128 = 2.07 waves 2457 Mbit/s); one wave of long windows
+  // spends the least on the guard warm-ups.
   const int64_t wave = static_cast<int64_t>(sm_count_) * kMinBlocks * kThreads;
-  for (int j = 2; j <= 4; ++j) {
+  for (int j = 1; j <= 4; ++j) {
     for (int w = std::max(guard, kGroup); w <= 1024; w += kGroup) {
       int64_t windows = 0;
       for (size_t i = 0; i < rq_in.n_cb; ++i) windows += (rq_in.cbs[i].k + w - 1) / w;
@@ -590,7 +591,7 @@ void Decoder::decode_plain(const DecodeRequest& rq) {
     d.work = work;
     d.out = rq.cbs[i].out_offset;
     work += k;
-    max_ckpt = std::max(max_ckpt, d.window / kSub);
+    max_ckpt = std::max(max_ckpt, d.window / kSub + 1);
     for (int w = 0; w < d.nwin; ++w) wincb.push_back(static_cast<int32_t>(i));
   }
   const int n_win = static_cast<int>(wincb.size());
@@ -623,7 +624,7 @@ void Decoder::decode_plain(const DecodeRequest& rq) {
     check(cudaMemsetAsync(post, 0, rq.post_len * sizeof(float), st), "zero posterior");
   }
   float4* ckpt = nullptr;
-  if (global_ckpt) ckpt = grow<float4>(d_ckpt_, static_cast<size_t>(n_win) * 2 * max_ckpt);
+  if (global_ckpt) ckpt = grow<float4>(d_ckpt_, ckpt_slab(n_win, 2 * static_cast<size_t>(max_ckpt)));
 
   upload(dcbs, cbs.data(), n * sizeof(DevCb), st);
   upload(dwin, wincb.data(), n_win * sizeof(int32_t), st);
@@ -781,7 +782,7 @@ void Decoder::decode_persistent(const DecodeRequest& rq) {
     d.work = work;
     d.out = rq.cbs[i].out_offset;
     work += k;
-    max_ckpt = std::max(max_ckpt, d.window / kSub);
+    max_ckpt = std::max(max_ckpt, d.window / kSub + 1);
   }
   // ---- tasks: blocks sorted by size, largest first, packed first-fit into 32 lanes ----
   std::vector<int32_t> order(n);
@@ -816,7 +817,7 @@ void Decoder::decode_persistent(const DecodeRequest& rq) {
   float* e1i = grow<float>(d_e1i_, work);
   float* e2 = grow<float>(d_e2_, work);
   float* seeds = grow<float>(d_seed_, static_cast<size_t>(n_win) * 16 * 4);
-  float4* ckpt = grow<float4>(d_ckpt_, static_cast<size_t>(n_win) * 2 * max_ckpt);
+  float4* ckpt = grow<float4>(d_ckpt_, ckpt_slab(n_win, 2 * static_cast<size_t>(max_ckpt)));
   uint8_t* done = grow<uint8_t>(d_done_, n);
   uint32_t* iters = (rq.device_memory && rq.iterations_used) ? rq.iterations_used
                                                               : grow<uint32_t>(d_iters_, n);

@@ -254,6 +254,15 @@ class Decoder {
   void take_error();  // throws DeviceTimeout (and clears the flag) if it is set; host-synchronous
 };
 
+// The kernels index a checkpoint slab (windows interleaved, siso.cuh CkptStrided) with 32-bit
+// plane offsets: a call whose slab would reach 2^31 float4 (32 GB) is refused.
+inline size_t ckpt_slab(size_t n_win, size_t planes) {
+  const size_t n = n_win * planes;
+  if (n >= (size_t{1} << 31))
+    throw CapacityExceeded("too many windows in one call for the checkpoint slab");
+  return n;
+}
+
 // Plain-schedule decode on the current device with all scratch in a fixed array of the library
 // image (noalloc.cu); device pointers in rq, ordered on rq.stream; never allocates.  Writes the
 // scratch bytes the request needs to *bytes_needed when given, and throws CapacityExceeded when

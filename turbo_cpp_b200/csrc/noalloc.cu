@@ -171,7 +171,7 @@ void decode_noalloc(const DecodeRequest& rq, size_t* bytes_needed) {
     d.work = work;
     d.out = rq.cbs[i].out_offset;
     work += k;
-    max_ckpt = std::max(max_ckpt, d.window / kSub);
+    max_ckpt = std::max(max_ckpt, d.window / kSub + 1);
     for (int w = 0; w < d.nwin; ++w) wincb.push_back(static_cast<int32_t>(i));
   }
   const int n_win = static_cast<int>(wincb.size());

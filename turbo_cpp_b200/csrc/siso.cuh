@@ -13,7 +13,7 @@
 // each, in shared memory or global scratch with the windows of a launch interleaved); the
 // backward pass recomputes the S alphas of one sub-window into registers from its checkpoint
 // and then runs beta + extrinsic over it.  The metrics are in the deferred-log (m, s) form of
-// trellis.cuh, normalised every 4 steps.
+// trellis.cuh.
 #pragma once
 #include <cstdint>
 
@@ -129,15 +129,17 @@ struct CkptGlobal {
 // pair per window, so the 32 lanes of a warp (consecutive windows) store and load 32
 // consecutive float4 -- four whole cache lines -- per instruction.
 struct CkptStrided {
-  float4* base;    // the launch's checkpoint slab
-  int64_t stride;  // windows of the launch (float4 pairs per plane)
-  int64_t g;       // this window
+  float4* p;     // this window's entry of plane 0
+  int stride;    // windows of the launch (float4 between planes); the host keeps the whole
+                 // slab below 2^31 float4
+  __device__ __forceinline__ CkptStrided(float4* base, int n_windows, int g)
+      : p(base + g), stride(n_windows) {}
   __device__ __forceinline__ void store(int j, const float (&m)[8]) const {
-    base[(2 * j) * stride + g] = make_float4(m[0], m[1], m[2], m[3]);
-    base[(2 * j + 1) * stride + g] = make_float4(m[4], m[5], m[6], m[7]);
+    p[(2 * j) * stride] = make_float4(m[0], m[1], m[2], m[3]);
+    p[(2 * j + 1) * stride] = make_float4(m[4], m[5], m[6], m[7]);
   }
   __device__ __forceinline__ void load(int j, float (&m)[8]) const {
-    const float4 x = base[(2 * j) * stride + g], y = base[(2 * j + 1) * stride + g];
+    const float4 x = p[(2 * j) * stride], y = p[(2 * j + 1) * stride];
     m[0] = x.x; m[1] = x.y; m[2] = x.z; m[3] = x.w; m[4] = y.x; m[5] = y.y; m[6] = y.z; m[7] = y.w;
   }
 };
@@ -209,23 +211,22 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
       }
       scale4(cur.lo, sa, a, b);
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        if (t == 3) alpha_step_ms<STD, true>(al, as, a[t], b[t]);
-        else alpha_step_ms<STD, false>(al, as, a[t], b[t]);
-      }
+      for (int t = 0; t < 4; ++t) alpha_step_ms<STD>(al, as, a[t], b[t]);
       if (q >= lo) {
         ms_to_log(al, as, v);
         ck.store((q - lo) / S + 1, v);
       }
       scale4(cur.hi, sa, a, b);
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        if (t == 3) alpha_step_ms<STD, true>(al, as, a[t], b[t]);
-        else alpha_step_ms<STD, false>(al, as, a[t], b[t]);
-      }
+      for (int t = 0; t < 4; ++t) alpha_step_ms<STD>(al, as, a[t], b[t]);
       ms_renorm(al, as);
       cur = nxt;
     }
+  }
+  if (!STD) {  // alpha at hi, the alpha_{t+1} of the window's last step
+    float v[8];
+    ms_to_log(al, as, v);
+    ck.store(nsub, v);
   }
   // seed for window w+1: alpha at hi - G
   if (w + 1 < cb.nwin && hi - G > 0) {
@@ -260,16 +261,10 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
       if (q - 8 >= hi) nxt = load_raw8<COHERENT>(sys, apr, par, q - 8);
       scale4(cur.hi, sa, a, b);
 #pragma unroll
-      for (int t = 3; t >= 0; --t) {
-        if (t == 0) beta_step_ms<STD, true>(be, bs, a[t], b[t]);
-        else beta_step_ms<STD, false>(be, bs, a[t], b[t]);
-      }
+      for (int t = 3; t >= 0; --t) beta_step_ms<STD>(be, bs, a[t], b[t]);
       scale4(cur.lo, sa, a, b);
 #pragma unroll
-      for (int t = 3; t >= 0; --t) {
-        if (t == 0) beta_step_ms<STD, true>(be, bs, a[t], b[t]);
-        else beta_step_ms<STD, false>(be, bs, a[t], b[t]);
-      }
+      for (int t = 3; t >= 0; --t) beta_step_ms<STD>(be, bs, a[t], b[t]);
       ms_renorm(be, bs);
       cur = nxt;
     }
@@ -290,12 +285,15 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
   Raw4 r_n;
   uint2 i_n;
   float c_n[8];
+  float an[8];  // reference code: alpha at base + S (log values), the last step's alpha_{t+1}
   if (nsub > 0) {
     const int base = lo + (nsub - 1) * S;
     r_n = load_raw4<COHERENT>(sys, apr, par, base);
     i_n = __ldg(reinterpret_cast<const uint2*>(pt + base));
     ck.load(nsub - 1, c_n);
+    if (!STD) ck.load(nsub, an);
   }
+  constexpr float kOnes[8] = {1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f};
   for (int j = nsub - 1; j >= 0; --j) {
     const int base = lo + j * S;
     const Raw4 r = r_n;
@@ -320,23 +318,36 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
         Al[t + 1][k] = Al[t][k];
         As[t + 1][k] = As[t][k];
       }
-      alpha_step_ms<STD, false>(Al[t + 1], As[t + 1], A_[t], B_[t]);
+      alpha_step_ms<STD>(Al[t + 1], As[t + 1], A_[t], B_[t]);
     }
     const uint32_t w2[2] = {iv.x, iv.y};
 #pragma unroll
     for (int t = S - 1; t >= 0; --t) {
-      const float e = io.scale * (kLn2 * extrinsic_ms<STD>(Al[t], As[t], be, bs, B_[t]));
+      // extrinsic (base 2): the reference's code from alpha_{t+1} beta_{t+1} (posterior minus
+      // Ls + La); the TS 36.212 code from alpha_t, gamma_t and beta_{t+1}
+      float e2;
+      if (STD)
+        e2 = extrinsic_ms<STD>(Al[t], As[t], be, bs, B_[t]);
+      else if (t == S - 1)
+        e2 = posterior_dest_ms(an, kOnes, be, bs) - 2.0f * A_[t];
+      else
+        e2 = posterior_dest_ms(Al[t + 1 < S ? t + 1 : t], As[t + 1 < S ? t + 1 : t], be, bs) -
+             2.0f * A_[t];
+      const float e = io.scale * (kLn2 * e2);
       const int n = static_cast<int>((w2[t >> 1] >> (16 * (t & 1))) & 0xffffu);
       io.ext[cb.work + n] = e;
       if (POST) io.post[cb.out + n] = SA[t] + e;
-      if (t == 0) beta_step_ms<STD, true>(be, bs, A_[t], B_[t]);
-      else beta_step_ms<STD, false>(be, bs, A_[t], B_[t]);
+      beta_step_ms<STD>(be, bs, A_[t], B_[t]);
       if (rec_beta && base + t == lo + G) {
         float rr[8];
         ms_to_log(be, bs, rr);
         bseed[0] = make_float4(rr[0], rr[1], rr[2], rr[3]);
         bseed[1] = make_float4(rr[4], rr[5], rr[6], rr[7]);
       }
+    }
+    if (!STD) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) an[k] = Al[0][k];
     }
     ms_renorm(be, bs);
   }

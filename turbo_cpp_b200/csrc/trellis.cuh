@@ -179,42 +179,46 @@ __device__ __forceinline__ void ms_join(float x, float y, float sx, float sy, fl
   m = fmaxf(x, y);
 }
 
-// alpha_{t+1} from alpha_t in (m, s) form; NORM: m normalised so that state 0's m is 0 (the
-// values are shift-invariant, so the recursions normalise only every few steps to bound m).
-template <bool STD = false, bool NORM = true>
+// alpha_{t+1} from alpha_t in (m, s) form.  The step subtracts state 0's incoming m through the
+// branch metrics (a - m0, -a - m0: two adds instead of eight), so the outgoing m stay within
+// one step's branch metric of each other's spread, as with a per-step normalisation; every
+// value is shift-invariant, so the offset left in m is never removed explicitly.
+template <bool STD = false>
 __device__ __forceinline__ void alpha_step_ms(float (&m)[8], float (&s)[8], float a, float b) {
-  const float g0 = a + b, g1 = a - b;
+  const float ap = a - m[0], am = -a - m[0];
   float mn[8], sn[8];
 #pragma unroll
   for (int n = 0; n < 8; ++n) {
     const int p0 = 2 * (n & 3);
-    ms_join(m[p0] + branch(pred_input<STD>(n, 0), pred_parity(n, 0), g0, g1),
-            m[p0 + 1] + branch(pred_input<STD>(n, 1), pred_parity(n, 1), g0, g1), s[p0],
-            s[p0 + 1], mn[n], sn[n]);
+    const int u0 = pred_input<STD>(n, 0), u1 = pred_input<STD>(n, 1);
+    const float bx = (u0 ? ap : am) + (pred_parity(n, 0) ? b : -b);
+    const float by = (u1 ? ap : am) + (pred_parity(n, 1) ? b : -b);
+    ms_join(m[p0] + bx, m[p0 + 1] + by, s[p0], s[p0 + 1], mn[n], sn[n]);
   }
-  const float r = NORM ? mn[0] : 0.0f;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) m[k] = NORM ? mn[k] - r : mn[k];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) s[k] = sn[k];
+  for (int k = 0; k < 8; ++k) {
+    m[k] = mn[k];
+    s[k] = sn[k];
+  }
 }
 
-// beta_t from beta_{t+1} in (m, s) form; NORM as for alpha_step_ms.
-template <bool STD = false, bool NORM = true>
+// beta_t from beta_{t+1} in (m, s) form, offset by state 0's incoming m as in alpha_step_ms.
+template <bool STD = false>
 __device__ __forceinline__ void beta_step_ms(float (&m)[8], float (&s)[8], float a, float b) {
-  const float g0 = a + b, g1 = a - b;
+  const float ap = a - m[0], am = -a - m[0];
   float mn[8], sn[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const int n0 = next_state<STD>(k, 0), n1 = next_state<STD>(k, 1);
-    ms_join(m[n0] + branch(0, parity<STD>(k, 0), g0, g1),
-            m[n1] + branch(1, parity<STD>(k, 1), g0, g1), s[n0], s[n1], mn[k], sn[k]);
+    const float bx = am + (parity<STD>(k, 0) ? b : -b);
+    const float by = ap + (parity<STD>(k, 1) ? b : -b);
+    ms_join(m[n0] + bx, m[n1] + by, s[n0], s[n1], mn[k], sn[k]);
   }
-  const float r = NORM ? mn[0] : 0.0f;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) m[k] = NORM ? mn[k] - r : mn[k];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) s[k] = sn[k];
+  for (int k = 0; k < 8; ++k) {
+    m[k] = mn[k];
+    s[k] = sn[k];
+  }
 }
 
 // Folds the binary exponent of each s (s >= 1) into its m, leaving s in [1, 2).
@@ -241,6 +245,32 @@ __device__ __forceinline__ void ms_to_log(const float (&m)[8], const float (&s)[
 __device__ __forceinline__ void ms_ones(float (&s)[8]) {
 #pragma unroll
   for (int k = 0; k < 8; ++k) s[k] = 1.0f;
+}
+
+// Posterior LLR (base 2) of step t of the reference's code from alpha_{t+1} and beta_{t+1} in
+// (m, s) form.  In that trellis the input of a branch is fixed by the state it enters
+// (u = n2^n1^n0, pred_input), so the log-sum over the u-branches of alpha_t + gamma_t +
+// beta_{t+1} equals the log-sum over the states n with that input of alpha_{t+1}(n) +
+// beta_{t+1}(n): two 4-way log-sums, each max + lg2(sum s_a s_b 2^(m - max)).  Any common shift
+// of alpha_{t+1} or beta_{t+1} cancels.  The extrinsic is this minus (Ls + La), as the reference
+// computes it (lte_turbo.cpp:483).  Not for the TS 36.212 code (its input depends on the
+// predecessor as well).
+__device__ __forceinline__ float posterior_dest_ms(const float (&ma)[8], const float (&sa)[8],
+                                                   const float (&mb)[8], const float (&sb)[8]) {
+  float v[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) v[n] = ma[n] + mb[n];
+  // states entered with input 1: {1, 2, 4, 7}; with input 0: {0, 3, 5, 6}
+  const float x1 = fmaxf(fmaxf(v[1], v[2]), fmaxf(v[4], v[7]));
+  const float x0 = fmaxf(fmaxf(v[0], v[3]), fmaxf(v[5], v[6]));
+  float s1 = 0.0f, s0 = 0.0f;
+#pragma unroll
+  for (int n = 0; n < 8; ++n) {
+    const float w = sa[n] * sb[n];
+    if (pred_input<false>(n, 0)) s1 = fmaf(w, ex2(v[n] - x1), s1);
+    else s0 = fmaf(w, ex2(v[n] - x0), s0);
+  }
+  return (x1 - x0) + (lg2(s1) - lg2(s0));
 }
 
 // Extrinsic LLR (base 2) of one step from alpha_t and beta_{t+1} in (m, s) form: the same
