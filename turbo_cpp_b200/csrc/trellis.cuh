@@ -16,6 +16,7 @@
 #pragma once
 #include <cstdint>
 
+
 namespace tcb {
 
 constexpr float kLog2e = 1.4426950408889634f;
@@ -179,46 +180,45 @@ __device__ __forceinline__ void ms_join(float x, float y, float sx, float sy, fl
   m = fmaxf(x, y);
 }
 
-// alpha_{t+1} from alpha_t in (m, s) form.  The step subtracts state 0's incoming m through the
-// branch metrics (a - m0, -a - m0: two adds instead of eight), so the outgoing m stay within
-// one step's branch metric of each other's spread, as with a per-step normalisation; every
-// value is shift-invariant, so the offset left in m is never removed explicitly.
+// alpha_{t+1} from alpha_t in (m, s) form; m normalised so that state 0's m is exactly 0.
+// (Subtracting state 0's incoming m through the branch metrics instead saves three adds per
+// step but was measured to lose float precision at LLR magnitudes in the tens of thousands.)
 template <bool STD = false>
 __device__ __forceinline__ void alpha_step_ms(float (&m)[8], float (&s)[8], float a, float b) {
-  const float ap = a - m[0], am = -a - m[0];
+  const float g0 = a + b, g1 = a - b;
   float mn[8], sn[8];
 #pragma unroll
   for (int n = 0; n < 8; ++n) {
     const int p0 = 2 * (n & 3);
-    const int u0 = pred_input<STD>(n, 0), u1 = pred_input<STD>(n, 1);
-    const float bx = (u0 ? ap : am) + (pred_parity(n, 0) ? b : -b);
-    const float by = (u1 ? ap : am) + (pred_parity(n, 1) ? b : -b);
-    ms_join(m[p0] + bx, m[p0 + 1] + by, s[p0], s[p0 + 1], mn[n], sn[n]);
+    ms_join(m[p0] + branch(pred_input<STD>(n, 0), pred_parity(n, 0), g0, g1),
+            m[p0 + 1] + branch(pred_input<STD>(n, 1), pred_parity(n, 1), g0, g1), s[p0],
+            s[p0 + 1], mn[n], sn[n]);
   }
+  const float r = mn[0];
+  m[0] = 0.0f;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    m[k] = mn[k];
-    s[k] = sn[k];
-  }
+  for (int k = 1; k < 8; ++k) m[k] = mn[k] - r;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s[k] = sn[k];
 }
 
-// beta_t from beta_{t+1} in (m, s) form, offset by state 0's incoming m as in alpha_step_ms.
+// beta_t from beta_{t+1} in (m, s) form; m normalised so that state 0's m is exactly 0.
 template <bool STD = false>
 __device__ __forceinline__ void beta_step_ms(float (&m)[8], float (&s)[8], float a, float b) {
-  const float ap = a - m[0], am = -a - m[0];
+  const float g0 = a + b, g1 = a - b;
   float mn[8], sn[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const int n0 = next_state<STD>(k, 0), n1 = next_state<STD>(k, 1);
-    const float bx = am + (parity<STD>(k, 0) ? b : -b);
-    const float by = ap + (parity<STD>(k, 1) ? b : -b);
-    ms_join(m[n0] + bx, m[n1] + by, s[n0], s[n1], mn[k], sn[k]);
+    ms_join(m[n0] + branch(0, parity<STD>(k, 0), g0, g1),
+            m[n1] + branch(1, parity<STD>(k, 1), g0, g1), s[n0], s[n1], mn[k], sn[k]);
   }
+  const float r = mn[0];
+  m[0] = 0.0f;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    m[k] = mn[k];
-    s[k] = sn[k];
-  }
+  for (int k = 1; k < 8; ++k) m[k] = mn[k] - r;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s[k] = sn[k];
 }
 
 // Folds the binary exponent of each s (s >= 1) into its m, leaving s in [1, 2).
