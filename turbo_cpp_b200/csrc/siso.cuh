@@ -168,6 +168,8 @@ __device__ __forceinline__ void tail_llrs(bool lower, const float* d0, int k, fl
   }
 }
 
+constexpr float kDestMaxA = 1024.0f;
+
 // Runs window w of block cb for one half-iteration.  g = launch-wide window index (seed slot).
 // lower: the SISO over interleaved order; post (lower SISO only): also write the posterior
 // Ls + e1 + e2 (last iteration, early stop).  Both may be compile-time constants (the plain
@@ -311,6 +313,11 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
     }
     float SA[S], A_[S], B_[S];
     scale4(r, SA, A_, B_);
+    // The alpha_{t+1} beta_{t+1} form subtracts Ls + La (2a) from a posterior of about that
+    // size, which costs float precision when |a| is huge; beyond kDestMaxA (base 2; ordinary
+    // decoding stays below ~300 even at 6 dB) the sub-window uses the branch form instead.
+    const bool dest = !STD && fmaxf(fmaxf(fabsf(A_[0]), fabsf(A_[1])),
+                                    fmaxf(fabsf(A_[2]), fabsf(A_[3]))) <= kDestMaxA;
 #pragma unroll
     for (int t = 0; t + 1 < S; ++t) {
 #pragma unroll
@@ -321,18 +328,8 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
       alpha_step_ms<STD>(Al[t + 1], As[t + 1], A_[t], B_[t]);
     }
     const uint32_t w2[2] = {iv.x, iv.y};
-#pragma unroll
-    for (int t = S - 1; t >= 0; --t) {
-      // extrinsic (base 2): the reference's code from alpha_{t+1} beta_{t+1} (posterior minus
-      // Ls + La); the TS 36.212 code from alpha_t, gamma_t and beta_{t+1}
-      float e2;
-      if (STD)
-        e2 = extrinsic_ms<STD>(Al[t], As[t], be, bs, B_[t]);
-      else if (t == S - 1)
-        e2 = posterior_dest_ms(an, kOnes, be, bs) - 2.0f * A_[t];
-      else
-        e2 = posterior_dest_ms(Al[t + 1 < S ? t + 1 : t], As[t + 1 < S ? t + 1 : t], be, bs) -
-             2.0f * A_[t];
+    // step t's outputs, then beta_t
+    auto finish = [&](int t, float e2) {
       const float e = io.scale * (kLn2 * e2);
       const int n = static_cast<int>((w2[t >> 1] >> (16 * (t & 1))) & 0xffffu);
       io.ext[cb.work + n] = e;
@@ -344,6 +341,15 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
         bseed[0] = make_float4(rr[0], rr[1], rr[2], rr[3]);
         bseed[1] = make_float4(rr[4], rr[5], rr[6], rr[7]);
       }
+    };
+    if (dest) {  // the reference's code: posterior from alpha_{t+1} beta_{t+1} minus Ls + La
+      finish(S - 1, posterior_dest_ms(an, kOnes, be, bs) - 2.0f * A_[S - 1]);
+#pragma unroll
+      for (int t = S - 2; t >= 0; --t)
+        finish(t, posterior_dest_ms(Al[t + 1], As[t + 1], be, bs) - 2.0f * A_[t]);
+    } else {  // the TS 36.212 code, and huge LLRs: from alpha_t, gamma_t and beta_{t+1}
+#pragma unroll
+      for (int t = S - 1; t >= 0; --t) finish(t, extrinsic_ms<STD>(Al[t], As[t], be, bs, B_[t]));
     }
     if (!STD) {
 #pragma unroll
