@@ -16,6 +16,7 @@
 // trellis.cuh.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 
 #include "trellis.cuh"
 
@@ -201,6 +202,7 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
     const float4 x = ld4_io<COHERENT>(io.seed_in + 16 * g), y = ld4_io<COHERENT>(io.seed_in + 16 * g + 4);
     al[0] = x.x; al[1] = x.y; al[2] = x.z; al[3] = x.w; al[4] = y.x; al[5] = y.y; al[6] = y.z; al[7] = y.w;
   }
+  float amax = 0.0f;  // largest |a| of the window (it covers [lo, hi))
   {  // 8-step groups (both halves of each sector); the next group is requested early
     Raw8 cur = load_raw8<COHERENT>(sys, apr, par, a_lo);
     for (int q = a_lo; q < hi; q += 8) {
@@ -212,6 +214,7 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
         ck.store((q - lo) / S, v);
       }
       scale4(cur.lo, sa, a, b);
+      amax = fmaxf(amax, fmaxf(fmaxf(fabsf(a[0]), fabsf(a[1])), fmaxf(fabsf(a[2]), fabsf(a[3]))));
 #pragma unroll
       for (int t = 0; t < 4; ++t) alpha_step_ms<STD>(al, as, a[t], b[t]);
       if (q >= lo) {
@@ -219,6 +222,7 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
         ck.store((q - lo) / S + 1, v);
       }
       scale4(cur.hi, sa, a, b);
+      amax = fmaxf(amax, fmaxf(fmaxf(fabsf(a[0]), fabsf(a[1])), fmaxf(fabsf(a[2]), fabsf(a[3]))));
 #pragma unroll
       for (int t = 0; t < 4; ++t) alpha_step_ms<STD>(al, as, a[t], b[t]);
       ms_renorm(al, as);
@@ -282,7 +286,13 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
 
   // ---- per 4-step sub-window (last to first): recompute alpha, then beta + extrinsic.  The
   // inputs, permutation indices and checkpoint of the next sub-window are requested one
-  // sub-window ahead. ----
+  // sub-window ahead.  The reference's code takes the extrinsic from alpha_{t+1} beta_{t+1}
+  // (DEST); that form subtracts Ls + La (2a) from a posterior of about that size, which costs
+  // float precision when |a| is huge, so a window whose |a| exceeds kDestMaxA (base 2; ordinary
+  // decoding stays below ~300 even at 6 dB) -- and the TS 36.212 code -- take the branch form.
+  // The two are separate copies of the loop, each with its own register allocation. ----
+  auto backward = [&](auto dest_tag) {
+  constexpr bool DEST = decltype(dest_tag)::value && !STD;
   const uint16_t* pt = (LOWER ? io.perm : io.inv) + cb.tab;
   Raw4 r_n;
   uint2 i_n;
@@ -293,7 +303,7 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
     r_n = load_raw4<COHERENT>(sys, apr, par, base);
     i_n = __ldg(reinterpret_cast<const uint2*>(pt + base));
     ck.load(nsub - 1, c_n);
-    if (!STD) ck.load(nsub, an);
+    if constexpr (DEST) ck.load(nsub, an);
   }
   constexpr float kOnes[8] = {1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f};
   for (int j = nsub - 1; j >= 0; --j) {
@@ -313,11 +323,6 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
     }
     float SA[S], A_[S], B_[S];
     scale4(r, SA, A_, B_);
-    // The alpha_{t+1} beta_{t+1} form subtracts Ls + La (2a) from a posterior of about that
-    // size, which costs float precision when |a| is huge; beyond kDestMaxA (base 2; ordinary
-    // decoding stays below ~300 even at 6 dB) the sub-window uses the branch form instead.
-    const bool dest = !STD && fmaxf(fmaxf(fabsf(A_[0]), fabsf(A_[1])),
-                                    fmaxf(fabsf(A_[2]), fabsf(A_[3]))) <= kDestMaxA;
 #pragma unroll
     for (int t = 0; t + 1 < S; ++t) {
 #pragma unroll
@@ -342,7 +347,7 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
         bseed[1] = make_float4(rr[4], rr[5], rr[6], rr[7]);
       }
     };
-    if (dest) {  // the reference's code: posterior from alpha_{t+1} beta_{t+1} minus Ls + La
+    if constexpr (DEST) {  // posterior from alpha_{t+1} beta_{t+1} minus Ls + La
       finish(S - 1, posterior_dest_ms(an, kOnes, be, bs) - 2.0f * A_[S - 1]);
 #pragma unroll
       for (int t = S - 2; t >= 0; --t)
@@ -351,12 +356,17 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
 #pragma unroll
       for (int t = S - 1; t >= 0; --t) finish(t, extrinsic_ms<STD>(Al[t], As[t], be, bs, B_[t]));
     }
-    if (!STD) {
+    if constexpr (DEST) {
 #pragma unroll
       for (int k = 0; k < 8; ++k) an[k] = Al[0][k];
     }
     ms_renorm(be, bs);
   }
+  };
+  if (!STD && amax <= kDestMaxA)
+    backward(std::true_type{});
+  else
+    backward(std::false_type{});
 }
 
 template <int S, bool LOWER, bool POST, class Ckpt, bool COHERENT = false, bool STD = false>

@@ -17,6 +17,7 @@
 #include <cstdint>
 
 
+
 namespace tcb {
 
 constexpr float kLog2e = 1.4426950408889634f;
@@ -35,6 +36,16 @@ __device__ __forceinline__ float lg2(float x) {
   float y;
   asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
+}
+
+// Three-input maximum (one sm_100 instruction) and the maximum of 8 values in four.
+__device__ __forceinline__ float max3(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ float max8(const float (&v)[8]) {
+  return fmaxf(max3(v[0], v[1], v[2]), max3(v[3], v[4], max3(v[5], v[6], v[7])));
 }
 
 // Jacobian logarithm in base 2: log2(2^x + 2^y).
@@ -180,9 +191,11 @@ __device__ __forceinline__ void ms_join(float x, float y, float sx, float sy, fl
   m = fmaxf(x, y);
 }
 
-// alpha_{t+1} from alpha_t in (m, s) form; m normalised so that state 0's m is exactly 0.
-// (Subtracting state 0's incoming m through the branch metrics instead saves three adds per
-// step but was measured to lose float precision at LLR magnitudes in the tens of thousands.)
+// alpha_{t+1} from alpha_t in (m, s) form; m normalised by its largest value, as the reference
+// normalises by the largest metric (lte_turbo.cpp:392-402): the likely states stay near 0,
+// where float rounding is finest.  (Normalising to state 0 instead puts every state at an
+// offset of state 0's metric, which on LLRs in the thousands was measured to cost the
+// precision of the likely states.)
 template <bool STD = false>
 __device__ __forceinline__ void alpha_step_ms(float (&m)[8], float (&s)[8], float a, float b) {
   const float g0 = a + b, g1 = a - b;
@@ -194,15 +207,15 @@ __device__ __forceinline__ void alpha_step_ms(float (&m)[8], float (&s)[8], floa
             m[p0 + 1] + branch(pred_input<STD>(n, 1), pred_parity(n, 1), g0, g1), s[p0],
             s[p0 + 1], mn[n], sn[n]);
   }
-  const float r = mn[0];
-  m[0] = 0.0f;
+  const float r = max8(mn);
 #pragma unroll
-  for (int k = 1; k < 8; ++k) m[k] = mn[k] - r;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) s[k] = sn[k];
+  for (int k = 0; k < 8; ++k) {
+    m[k] = mn[k] - r;
+    s[k] = sn[k];
+  }
 }
 
-// beta_t from beta_{t+1} in (m, s) form; m normalised so that state 0's m is exactly 0.
+// beta_t from beta_{t+1} in (m, s) form; m normalised by its largest value.
 template <bool STD = false>
 __device__ __forceinline__ void beta_step_ms(float (&m)[8], float (&s)[8], float a, float b) {
   const float g0 = a + b, g1 = a - b;
@@ -213,12 +226,12 @@ __device__ __forceinline__ void beta_step_ms(float (&m)[8], float (&s)[8], float
     ms_join(m[n0] + branch(0, parity<STD>(k, 0), g0, g1),
             m[n1] + branch(1, parity<STD>(k, 1), g0, g1), s[n0], s[n1], mn[k], sn[k]);
   }
-  const float r = mn[0];
-  m[0] = 0.0f;
+  const float r = max8(mn);
 #pragma unroll
-  for (int k = 1; k < 8; ++k) m[k] = mn[k] - r;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) s[k] = sn[k];
+  for (int k = 0; k < 8; ++k) {
+    m[k] = mn[k] - r;
+    s[k] = sn[k];
+  }
 }
 
 // Folds the binary exponent of each s (s >= 1) into its m, leaving s in [1, 2).
@@ -232,14 +245,14 @@ __device__ __forceinline__ void ms_renorm(float (&m)[8], float (&s)[8]) {
   }
 }
 
-// (m, s) -> log values m + lg2(s), normalised so that state 0 is 0.
+// (m, s) -> log values m + lg2(s), normalised by their largest value.
 __device__ __forceinline__ void ms_to_log(const float (&m)[8], const float (&s)[8], float (&v)[8]) {
   float r[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) r[k] = m[k] + lg2(s[k]);
-  v[0] = 0.0f;
+  const float x = max8(r);
 #pragma unroll
-  for (int k = 1; k < 8; ++k) v[k] = r[k] - r[0];
+  for (int k = 0; k < 8; ++k) v[k] = r[k] - x;
 }
 
 __device__ __forceinline__ void ms_ones(float (&s)[8]) {
@@ -261,8 +274,8 @@ __device__ __forceinline__ float posterior_dest_ms(const float (&ma)[8], const f
 #pragma unroll
   for (int n = 0; n < 8; ++n) v[n] = ma[n] + mb[n];
   // states entered with input 1: {1, 2, 4, 7}; with input 0: {0, 3, 5, 6}
-  const float x1 = fmaxf(fmaxf(v[1], v[2]), fmaxf(v[4], v[7]));
-  const float x0 = fmaxf(fmaxf(v[0], v[3]), fmaxf(v[5], v[6]));
+  const float x1 = fmaxf(max3(v[1], v[2], v[4]), v[7]);
+  const float x0 = fmaxf(max3(v[0], v[3], v[5]), v[6]);
   float s1 = 0.0f, s0 = 0.0f;
 #pragma unroll
   for (int n = 0; n < 8; ++n) {
@@ -285,10 +298,7 @@ __device__ __forceinline__ float extrinsic_ms(const float (&ma)[8], const float 
     m0[k] = ma[k] + mb[next_state<STD>(k, 0)] + (parity<STD>(k, 0) ? b : -b);
     m1[k] = ma[k] + mb[next_state<STD>(k, 1)] + (parity<STD>(k, 1) ? b : -b);
   }
-  const float x0 = fmaxf(fmaxf(fmaxf(m0[0], m0[1]), fmaxf(m0[2], m0[3])),
-                         fmaxf(fmaxf(m0[4], m0[5]), fmaxf(m0[6], m0[7])));
-  const float x1 = fmaxf(fmaxf(fmaxf(m1[0], m1[1]), fmaxf(m1[2], m1[3])),
-                         fmaxf(fmaxf(m1[4], m1[5]), fmaxf(m1[6], m1[7])));
+  const float x0 = max8(m0), x1 = max8(m1);
   float s0 = 0.0f, s1 = 0.0f;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
