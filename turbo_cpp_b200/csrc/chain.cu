@@ -253,14 +253,15 @@ void Decoder::decode_transport_blocks(const TbRequest& q) {
     r.host_async = false;
     r.stream = nullptr;  // the worker's own stream
     const uint64_t launches_before = w.timing_.launches;
-    w.transport_blocks(r, false);
+    w.transport_blocks(r, false, last_compute_, w.compute_event());
+    last_compute_ = w.compute_done_;
     timing_.launches += w.timing_.launches - launches_before;
     return;
   }
   transport_blocks(q, true);
 }
 
-void Decoder::transport_blocks(const TbRequest& q, bool wait) {
+void Decoder::transport_blocks(const TbRequest& q, bool wait, void* after, void* done) {
   std::lock_guard<std::mutex> lock(mu_);
   check(cudaSetDevice(device_), "cudaSetDevice");
   cudaStream_t st = static_cast<cudaStream_t>(q.device_memory ? q.stream
@@ -303,6 +304,7 @@ void Decoder::transport_blocks(const TbRequest& q, bool wait) {
           "copy rate-matched LLRs in");
     e_llr = de;
   }
+  if (after) check(cudaStreamWaitEvent(st, static_cast<cudaEvent_t>(after), 0), "cudaStreamWaitEvent");
   float* d012 = grow<float>(d_d012_, static_cast<size_t>(llr_len));
   float* post = grow<float>(d_tbpost_, static_cast<size_t>(post_len));
   uint8_t* bits = q.device_memory ? q.bits : grow<uint8_t>(d_tbbits_, q.bits_len);
@@ -373,6 +375,7 @@ void Decoder::transport_blocks(const TbRequest& q, bool wait) {
     return;
   }
   body();
+  if (done) check(cudaEventRecord(static_cast<cudaEvent_t>(done), st), "cudaEventRecord");
   if (!q.device_memory) {
     check(cudaMemcpyAsync(q.bits, bits, static_cast<size_t>(bits_len), cudaMemcpyDeviceToHost, st),
           "copy bits out");

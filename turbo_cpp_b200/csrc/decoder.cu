@@ -170,6 +170,7 @@ Decoder::~Decoder() {
   cudaSetDevice(device_);
   for (auto& g : graphs_) drop_graph(g);
   if (last_event_) cudaEventDestroy(static_cast<cudaEvent_t>(last_event_));
+  if (compute_done_) cudaEventDestroy(static_cast<cudaEvent_t>(compute_done_));
   d_err_.release();
   for (auto& e : events_) {
     if (e.start) cudaEventDestroy(static_cast<cudaEvent_t>(e.start));
@@ -692,6 +693,15 @@ void Decoder::decode_plain(const DecodeRequest& rq) {
 // ------------------------------------------------------------------------------------------
 // Asynchronous host-memory calls
 // ------------------------------------------------------------------------------------------
+void* Decoder::compute_event() {
+  if (!compute_done_) {
+    cudaEvent_t e;
+    check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    compute_done_ = e;
+  }
+  return compute_done_;
+}
+
 void Decoder::decode_host_async(const DecodeRequest& rq) {
   if (rq.n_cb == 0) return;
   check(cudaSetDevice(device_), "cudaSetDevice");
@@ -721,7 +731,12 @@ void Decoder::decode_host_async(const DecodeRequest& rq) {
   r.graph = false;
   r.auto_schedule = false;
   r.stream = ws;
+  // the decode follows the previous call's decode (another worker); the copy-in above does not
+  if (last_compute_)
+    check(cudaStreamWaitEvent(ws, static_cast<cudaEvent_t>(last_compute_), 0), "cudaStreamWaitEvent");
   if (r.persistent) w.decode_persistent(r); else w.decode_plain(r);
+  check(cudaEventRecord(static_cast<cudaEvent_t>(w.compute_event()), ws), "cudaEventRecord");
+  last_compute_ = w.compute_done_;
   check(cudaMemcpyAsync(rq.posterior, dp, rq.post_len * sizeof(float), cudaMemcpyDeviceToHost, ws),
         "copy posterior out");
   if (rq.crc_ok)

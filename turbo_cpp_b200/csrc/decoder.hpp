@@ -183,7 +183,11 @@ class Decoder {
   // Asynchronous host-memory calls rotate over kAsyncWorkers worker decoders, each with its own
   // device buffers and stream: a call enqueues copy-in, decode and copy-out on the next worker
   // and returns, so that its copies run while the previous calls decode.  sync() waits for them.
-  void transport_blocks(const TbRequest& q, bool wait);  // wait: synchronise host-memory calls
+  // wait: synchronise host-memory calls; after/done (cudaEvent_t, may be null): the chain's
+  // device work waits for `after` once its inputs are copied in and records `done` before its
+  // outputs are copied out
+  void transport_blocks(const TbRequest& q, bool wait, void* after = nullptr,
+                        void* done = nullptr);
   void decode_host_async(const DecodeRequest& rq);
   std::vector<std::unique_ptr<Decoder>> workers_;
   size_t next_worker_ = 0;
@@ -249,6 +253,11 @@ class Decoder {
   DeviceBuffer d_err_;          // sticky: set by a persistent-schedule wait that gave up
   int stall_task_ = -1;
   void* last_event_ = nullptr;  // completion of the previous decode (orders workspace reuse)
+  // Host-async calls: the decode of each call waits for the previous call's decode (on another
+  // worker), so that decodes run one at a time on the whole GPU while copies overlap them.
+  void* compute_done_ = nullptr;  // worker: end of its latest call's device compute
+  void* last_compute_ = nullptr;  // caller: the latest worker's compute_done_ event
+  void* compute_event();          // this decoder's compute_done_ (created on first use)
   void order_after_previous(void* stream);
   void mark_done(void* stream);
   void take_error();  // throws DeviceTimeout (and clears the flag) if it is set; host-synchronous
