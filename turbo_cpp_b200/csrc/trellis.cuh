@@ -191,45 +191,47 @@ __device__ __forceinline__ void ms_join(float x, float y, float sx, float sy, fl
   m = fmaxf(x, y);
 }
 
-// alpha_{t+1} from alpha_t in (m, s) form; m normalised by its largest value, as the reference
-// normalises by the largest metric (lte_turbo.cpp:392-402): the likely states stay near 0,
-// where float rounding is finest.  (Normalising to state 0 instead puts every state at an
-// offset of state 0's metric, which on LLRs in the thousands was measured to cost the
-// precision of the likely states.)
+// alpha_{t+1} from alpha_t in (m, s) form, normalised by the largest incoming metric, as the
+// reference normalises by the largest metric (lte_turbo.cpp:392-402): the likely states stay
+// near 0, where float rounding is finest.  The normalisation goes through the branch metrics
+// (a - r, -a - r with r = max(m), sm_100's three-input max.f32: 10 instructions instead of a
+// 14-instruction normalisation of the outputs); every value is shift-invariant.  (Normalising
+// to state 0 instead puts the likely states at state 0's offset, which on LLRs in the
+// thousands was measured to cost their precision.)
 template <bool STD = false>
 __device__ __forceinline__ void alpha_step_ms(float (&m)[8], float (&s)[8], float a, float b) {
-  const float g0 = a + b, g1 = a - b;
+  const float r = max8(m);
+  const float ap = a - r, am = -a - r;
   float mn[8], sn[8];
 #pragma unroll
   for (int n = 0; n < 8; ++n) {
     const int p0 = 2 * (n & 3);
-    ms_join(m[p0] + branch(pred_input<STD>(n, 0), pred_parity(n, 0), g0, g1),
-            m[p0 + 1] + branch(pred_input<STD>(n, 1), pred_parity(n, 1), g0, g1), s[p0],
-            s[p0 + 1], mn[n], sn[n]);
+    const float bx = (pred_input<STD>(n, 0) ? ap : am) + (pred_parity(n, 0) ? b : -b);
+    const float by = (pred_input<STD>(n, 1) ? ap : am) + (pred_parity(n, 1) ? b : -b);
+    ms_join(m[p0] + bx, m[p0 + 1] + by, s[p0], s[p0 + 1], mn[n], sn[n]);
   }
-  const float r = max8(mn);
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    m[k] = mn[k] - r;
+    m[k] = mn[k];
     s[k] = sn[k];
   }
 }
 
-// beta_t from beta_{t+1} in (m, s) form; m normalised by its largest value.
+// beta_t from beta_{t+1} in (m, s) form, normalised through the branch metrics as alpha_step_ms.
 template <bool STD = false>
 __device__ __forceinline__ void beta_step_ms(float (&m)[8], float (&s)[8], float a, float b) {
-  const float g0 = a + b, g1 = a - b;
+  const float r = max8(m);
+  const float ap = a - r, am = -a - r;
   float mn[8], sn[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const int n0 = next_state<STD>(k, 0), n1 = next_state<STD>(k, 1);
-    ms_join(m[n0] + branch(0, parity<STD>(k, 0), g0, g1),
-            m[n1] + branch(1, parity<STD>(k, 1), g0, g1), s[n0], s[n1], mn[k], sn[k]);
+    ms_join(m[n0] + (am + (parity<STD>(k, 0) ? b : -b)),
+            m[n1] + (ap + (parity<STD>(k, 1) ? b : -b)), s[n0], s[n1], mn[k], sn[k]);
   }
-  const float r = max8(mn);
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    m[k] = mn[k] - r;
+    m[k] = mn[k];
     s[k] = sn[k];
   }
 }
