@@ -790,9 +790,14 @@ def main():
             "avg_launch_ms": avg_launch_ms,
             "peak_source": f"{props.multi_processor_count} SMs x {MUFU_PER_SM_CLK} MUFU/clk x "
                            f"median sampled SM clock {sm_mhz:.0f} MHz (nominal issue rate)",
-            "note": "the binding roofline is the SFU (MUFU ex2/lg2 of the exact max*); the "
-                    "trellis is not a contraction (no tensor cores) and HBM runs well below its "
-                    "measured peak (roofline_hbm)",
+            "note": "achieved counts the reference formulation's work, 60 transcendentals per "
+                    "trellis step (30 exact max*, each an exp and a log1p), against the MUFU "
+                    "issue rate; the kernel's deferred-log arithmetic executes about 43 MUFU ops "
+                    "per output step (one ex2 per max* in the recursions, two 4-way log-sums for "
+                    "the extrinsic), so what binds is instruction issue (ncu: issue 69 % busy, "
+                    "XU 53 %, ~460 instructions per output step; "
+                    "profiles/siso_plain_kernel_k6144x4096.md); no tensor cores (not a "
+                    "contraction); HBM well below its peak (roofline_hbm)",
         },
         "roofline_hbm": {
             "bound": "hbm", "achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
