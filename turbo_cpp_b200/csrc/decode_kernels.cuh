@@ -205,7 +205,10 @@ __global__ void __launch_bounds__(kPersistThreads, kPersistMinBlocks)
                     : SisoIo{p.llr, p.sys_i, p.e1i, p.e2, p.post, p.perm, p.inv, p.seed_lo[it & 1],
                              p.seed_lo[(it + 1) & 1], p.scale[2 * it + 1], p.guard};
       if (active)
-        siso_window_rt<kSub, decltype(ck), true, STD>(cb, w, g, io, ck, half == 1,
+        // 4-step loop bodies: the one SISO copy for both halves plus the queue, CRC and wait
+        // code must fit the instruction cache (measured 3166 against 2830 Mbit/s with 8-step
+        // bodies at 4096 x K=6144, window 192; the plain kernels keep 8-step bodies)
+        siso_window_rt<kSub, decltype(ck), true, STD, true>(cb, w, g, io, ck, half == 1,
                                                     half == 1 && post_now);
       if (half == 1 && p.early_stop) {
         // CRC24B syndrome of the hard decisions (lte_turbo.cpp:792-804): each lane XORs

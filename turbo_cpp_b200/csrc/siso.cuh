@@ -177,7 +177,7 @@ constexpr float kDestMaxA = 1024.0f;
 // kernels, one specialisation each) or run-time values (the persistent kernel, which keeps a
 // single copy of this code for both halves).  COHERENT: a-priori and seeds were written earlier
 // in the same kernel (persistent schedule).
-template <int S, class Ckpt, bool COHERENT, bool STD = false>
+template <int S, class Ckpt, bool COHERENT, bool STD = false, bool SMALL_LOOPS = false>
 __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, const SisoIo& io,
                                                const Ckpt& ck, const bool LOWER, const bool POST) {
   static_assert(S == 4, "sub-windows are one float4 group of 4 steps");
@@ -203,7 +203,24 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
     al[0] = x.x; al[1] = x.y; al[2] = x.z; al[3] = x.w; al[4] = y.x; al[5] = y.y; al[6] = y.z; al[7] = y.w;
   }
   float amax = 0.0f;  // largest |a| of the window (it covers [lo, hi))
-  {  // 8-step groups (both halves of each sector); the next group is requested early
+  if constexpr (SMALL_LOOPS) {  // 4-step groups; the next group is requested early
+    Raw4 cur = load_raw4<COHERENT>(sys, apr, par, a_lo);
+    for (int q = a_lo; q < hi; q += 4) {
+      Raw4 nxt = cur;
+      if (q + 4 < hi) nxt = load_raw4<COHERENT>(sys, apr, par, q + 4);
+      if (q >= lo) {
+        float v[8];
+        ms_to_log(al, as, v);
+        ck.store((q - lo) / S, v);
+      }
+      scale4(cur, sa, a, b);
+      amax = fmaxf(amax, fmaxf(fmaxf(fabsf(a[0]), fabsf(a[1])), fmaxf(fabsf(a[2]), fabsf(a[3]))));
+#pragma unroll
+      for (int t = 0; t < 4; ++t) alpha_step_ms<STD>(al, as, a[t], b[t]);
+      ms_renorm(al, as);
+      cur = nxt;
+    }
+  } else {  // 8-step groups (both halves of each sector); the next group is requested early
     Raw8 cur = load_raw8<COHERENT>(sys, apr, par, a_lo);
     for (int q = a_lo; q < hi; q += 8) {
       Raw8 nxt = cur;
@@ -260,7 +277,19 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
     const float4 x = ld4_io<COHERENT>(io.seed_in + 16 * g + 8), y = ld4_io<COHERENT>(io.seed_in + 16 * g + 12);
     be[0] = x.x; be[1] = x.y; be[2] = x.z; be[3] = x.w; be[4] = y.x; be[5] = y.y; be[6] = y.z; be[7] = y.w;
   }
-  if (b_hi > hi) {
+  if (SMALL_LOOPS && b_hi > hi) {
+    Raw4 cur = load_raw4<COHERENT>(sys, apr, par, b_hi - 4);
+    for (int q = b_hi - 4; q >= hi; q -= 4) {
+      Raw4 nxt = cur;
+      if (q - 4 >= hi) nxt = load_raw4<COHERENT>(sys, apr, par, q - 4);
+      scale4(cur, sa, a, b);
+#pragma unroll
+      for (int t = 3; t >= 0; --t) beta_step_ms<STD>(be, bs, a[t], b[t]);
+      ms_renorm(be, bs);
+      cur = nxt;
+    }
+  }
+  if (!SMALL_LOOPS && b_hi > hi) {
     Raw8 cur = load_raw8<COHERENT>(sys, apr, par, b_hi - 8);
     for (int q = b_hi - 8; q >= hi; q -= 8) {
       Raw8 nxt = cur;
