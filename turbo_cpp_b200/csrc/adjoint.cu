@@ -138,6 +138,33 @@ __device__ __forceinline__ float ext_weights(const float (&al)[8], const float (
   return WANT_VALUE ? (x1 - x0) + (lg2(s1) - lg2(s0)) : 0.0f;
 }
 
+// The reference code's extrinsic in the destination form of the forward decoder (trellis.cuh
+// posterior_dest_ms): F = log-sum over the states entered with input 1 of alpha_{t+1} +
+// beta_{t+1} minus the same over input 0, and the extrinsic is F - 2a.  w[n] = dF/d alpha_{t+1}(n)
+// = dF/d beta_{t+1}(n): the softmax weight of state n within its side, positive for input 1,
+// negative for input 0 (8 ex2 + 2 rcp instead of 16 ex2 + 2 rcp for the branch form).  alpha may
+// be in (m, s) form (sa, log values when all 1); beta in log values.  Returns F when WANT_VALUE.
+template <bool WANT_VALUE>
+__device__ __forceinline__ float dest_weights(const float (&ma)[8], const float (&sa)[8],
+                                              const float (&mb)[8], float (&w)[8]) {
+  float v[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) v[n] = ma[n] + mb[n];
+  const float x1 = fmaxf(max3(v[1], v[2], v[4]), v[7]);
+  const float x0 = fmaxf(max3(v[0], v[3], v[5]), v[6]);
+  float s1 = 0.0f, s0 = 0.0f;
+#pragma unroll
+  for (int n = 0; n < 8; ++n) {
+    const bool one = pred_input<false>(n, 0);
+    w[n] = sa[n] * ex2(v[n] - (one ? x1 : x0));
+    if (one) s1 += w[n]; else s0 += w[n];
+  }
+  const float r1 = rcp(s1), r0 = rcp(s0);
+#pragma unroll
+  for (int n = 0; n < 8; ++n) w[n] *= pred_input<false>(n, 0) ? r1 : -r0;
+  return WANT_VALUE ? (x1 - x0) + (lg2(s1) - lg2(s0)) : 0.0f;
+}
+
 struct AdjIo {
   const float* llr;       // channel LLRs, [d0|d1|d2] per block
   const float* sys_i;     // interleaved systematic LLRs (work layout)
@@ -207,14 +234,24 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
   const float xs = kLn2 * io.scale;  // d e / d(base-2 extrinsic)
 
   if (PHASES & 1) {
-  // ---- A: alpha checkpoints at a_lo + 4m ----
-  float al[8];
+  // ---- A: alpha checkpoints (log values) at a_lo + 4m; the recursion itself runs in the
+  // deferred-log (m, s) form of the forward decoder (one ex2 per max*) ----
+  float al[8], as[8];
+  ms_ones(as);
   if (start) alpha_start(al); else load8(io.seeds + 16 * g, al);
   for (int q = a_lo; q < hi; q += 4) {
-    cka.store((q - a_lo) >> 2, al);
+    float v[8];
+    ms_to_log(al, as, v);
+    cka.store((q - a_lo) >> 2, v);
     scale4(load_raw4(sys, apr, par, q), sa, a, b);
 #pragma unroll
-    for (int t = 0; t < 4; ++t) alpha_step<STD>(al, a[t], b[t]);
+    for (int t = 0; t < 4; ++t) alpha_step_ms<STD>(al, as, a[t], b[t]);
+    ms_renorm(al, as);
+  }
+  if (!STD) {  // alpha at hi: the alpha_{t+1} of the window's last step (destination form)
+    float v[8];
+    ms_to_log(al, as, v);
+    cka.store((hi - a_lo) >> 2, v);
   }
 
   // ---- B: backward in time ----
@@ -226,16 +263,30 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
   } else {
     load8(io.seeds + 16 * g + 8, be);
   }
-  for (int P = b_hi; P > hi; P -= 4) {  // beta warm-up: checkpoints at lo + 4m
-    ckb.store((P - lo) >> 2, be);
-    scale4(load_raw4(sys, apr, par, P - 4), sa, a, b);
+  {  // beta warm-up in (m, s) form: checkpoints (log values) at lo + 4m
+    float bs[8];
+    ms_ones(bs);
+    for (int P = b_hi; P > hi; P -= 4) {
+      float v[8];
+      ms_to_log(be, bs, v);
+      ckb.store((P - lo) >> 2, v);
+      scale4(load_raw4(sys, apr, par, P - 4), sa, a, b);
 #pragma unroll
-    for (int t = 3; t >= 0; --t) beta_step<STD>(be, a[t], b[t]);
+      for (int t = 3; t >= 0; --t) beta_step_ms<STD>(be, bs, a[t], b[t]);
+      ms_renorm(be, bs);
+    }
+    float v[8];
+    ms_to_log(be, bs, v);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) be[k] = v[k];
   }
   float ab[8];
 #pragma unroll
   for (int s = 0; s < 8; ++s) ab[s] = 0.0f;
   float spart = 0.0f;
+  float an[8];  // reference code: alpha at P (log values), the last step's alpha_{t+1}
+  if (!STD) cka.load((hi - a_lo) >> 2, an);
+  constexpr float kOnes[8] = {1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f};
   for (int P = hi; P > lo; P -= 4) {  // the window's own steps
     ckb.store((P - lo) >> 2, be);
     const int q = P - 4;
@@ -253,15 +304,27 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
     float gsa[4], gpar[4];
 #pragma unroll
     for (int t = 3; t >= 0; --t) {
-      float w0[8], w1[8];
-      const float d2 = ext_weights<true, STD>(Al[t], be, b[t], w0, w1);
-      spart += ge[t] * (kLn2 * d2);
       const float G2 = xs * ge[t];
       float nab[8], ga = 0.0f, gb = 0.0f;
+      if constexpr (!STD) {  // destination form: direct adjoint on alpha_{t+1}, -2 on a_t
+        float w[8];
+        const float F = dest_weights<true>(t == 3 ? an : Al[t < 3 ? t + 1 : t], kOnes, be, w);
+        spart += ge[t] * (kLn2 * (F - 2.0f * a[t]));
 #pragma unroll
-      for (int s = 0; s < 8; ++s) {
-        nab[s] = G2 * (w1[s] - w0[s]);
-        gb += G2 * ((parity<STD>(s, 1) ? w1[s] : -w1[s]) - (parity<STD>(s, 0) ? w0[s] : -w0[s]));
+        for (int s = 0; s < 8; ++s) {
+          ab[s] += G2 * w[s];
+          nab[s] = 0.0f;
+        }
+        ga = -2.0f * G2;
+      } else {
+        float w0[8], w1[8];
+        const float d2 = ext_weights<true, STD>(Al[t], be, b[t], w0, w1);
+        spart += ge[t] * (kLn2 * d2);
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+          nab[s] = G2 * (w1[s] - w0[s]);
+          gb += G2 * ((parity<STD>(s, 1) ? w1[s] : -w1[s]) - (parity<STD>(s, 0) ? w0[s] : -w0[s]));
+        }
       }
       alpha_adjoint<STD>(Al[t], a[t], b[t], ab, nab, ga, gb);
 #pragma unroll
@@ -272,6 +335,10 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
     }
     *reinterpret_cast<float4*>(io.own_sa + cb.work + q) = make_float4(gsa[0], gsa[1], gsa[2], gsa[3]);
     *reinterpret_cast<float4*>(io.own_par + cb.work + q) = make_float4(gpar[0], gpar[1], gpar[2], gpar[3]);
+    if (!STD) {
+#pragma unroll
+      for (int s = 0; s < 8; ++s) an[s] = Al[0][s];
+    }
   }
   for (int P = lo; P > a_lo; P -= 4) {  // alpha warm-up steps
     const int q = P - 4;
@@ -305,9 +372,10 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
 
   if (PHASES & 2) {
   // ---- C: forward in time ----
-  float bb[8], al[8];
+  float bb[8], al[8], as[8];  // alpha in (m, s) form, advanced over the window's own steps
 #pragma unroll
   for (int s = 0; s < 8; ++s) bb[s] = 0.0f;
+  ms_ones(as);
   cka.load((lo - a_lo) >> 2, al);
   float* bg = ag + 2 * G;
   for (int P = lo; P < b_hi; P += 4) {
@@ -331,21 +399,32 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
       for (int s = 0; s < 8; ++s) nbb[s] = 0.0f;
       beta_adjoint<STD>(Bt[t], a[t], b[t], bb, nbb, ga, gb);
       if (own) {
-        float w0[8], w1[8];
-        ext_weights<false, STD>(al, Bt[t], b[t], w0, w1);
         const float G2 = xs * ge[t];
+        if constexpr (!STD) {  // destination form: direct adjoint on beta_{t+1}
+          alpha_step_ms<STD>(al, as, a[t], b[t]);  // alpha_{t+1}
+          float w[8];
+          dest_weights<false>(al, as, Bt[t], w);
 #pragma unroll
-        for (int s = 0; s < 8; ++s) {
-          nbb[next_state<STD>(s, 0)] -= G2 * w0[s];
-          nbb[next_state<STD>(s, 1)] += G2 * w1[s];
+          for (int s = 0; s < 8; ++s) nbb[s] += G2 * w[s];
+        } else {
+          float w0[8], w1[8];
+          float lal[8];
+          ms_to_log(al, as, lal);
+          ext_weights<false, STD>(lal, Bt[t], b[t], w0, w1);
+#pragma unroll
+          for (int s = 0; s < 8; ++s) {
+            nbb[next_state<STD>(s, 0)] -= G2 * w0[s];
+            nbb[next_state<STD>(s, 1)] += G2 * w1[s];
+          }
+          alpha_step_ms<STD>(al, as, a[t], b[t]);
         }
-        alpha_step<STD>(al, a[t], b[t]);
       }
 #pragma unroll
       for (int s = 0; s < 8; ++s) bb[s] = nbb[s];
       gsa[t] = kHalfLog2e * ga;
       gpar[t] = kHalfLog2e * gb;
     }
+    ms_renorm(al, as);
     if (own) {
       float4* ps = reinterpret_cast<float4*>(io.own_sa + cb.work + P);
       float4* pp = reinterpret_cast<float4*>(io.own_par + cb.work + P);
