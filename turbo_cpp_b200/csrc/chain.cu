@@ -42,15 +42,18 @@ __global__ void __launch_bounds__(kRmThreads) derate_llr_kernel(const DevRm* __r
   const DevRm b = blocks[blockIdx.x];
   CircularScan cs(b.k, b.filler);
   float* out = d012 + b.out;
-  for (int i = threadIdx.x; i < 3 * cs.d; i += blockDim.x) out[i] = 0.0f;
+  // every position of [d0|d1|d2] is a valid buffer position, written below, except the filler
+  // positions of d0 and d1 (<NULL> in the buffer), which de-rate matching sets to 0
+  for (int i = threadIdx.x; i < cs.filler; i += blockDim.x) out[i] = out[cs.d + i] = 0.0f;
   cs.scan(warp_sum, &s_total);
   cs.rank_of(cs.k0(b.rv), &s_rank_k0);
-  __syncthreads();  // also orders the zero fill before the scattered writes
+  __syncthreads();
   const int nv = s_total, r0 = s_rank_k0;
   const float* x = e_llr + b.e_off;
   int rank = cs.before;
+  CircularWalk wk = cs.walk(cs.p0);
   for (int p = cs.p0; p < cs.p1; ++p) {
-    const int src = cs.source(p);
+    const int src = wk.next();
     if (src < 0) continue;
     int kk = rank - r0;
     if (kk < 0) kk += nv;
@@ -79,14 +82,17 @@ __global__ void __launch_bounds__(kRmThreads) derate_combine_kernel(
   const DevRm b = tx[t0];
   CircularScan cs(b.k, b.filler);
   float* out = d012 + b.out;
-  for (int i = threadIdx.x; i < 3 * cs.d; i += blockDim.x) out[i] = 0.0f;
+  // every position of [d0|d1|d2] is a valid buffer position, written below, except the filler
+  // positions of d0 and d1 (<NULL> in the buffer), which de-rate matching sets to 0
+  for (int i = threadIdx.x; i < cs.filler; i += blockDim.x) out[i] = out[cs.d + i] = 0.0f;
   cs.scan(warp_sum, &s_total);
   for (int t = 0; t < nt; ++t) cs.rank_of(cs.k0(tx[t0 + t].rv), &s_rank_k0[t]);
-  __syncthreads();  // also orders the zero fill before the scattered writes
+  __syncthreads();
   const int nv = s_total;
   int rank = cs.before;
+  CircularWalk wk = cs.walk(cs.p0);
   for (int p = cs.p0; p < cs.p1; ++p) {
-    const int src = cs.source(p);
+    const int src = wk.next();
     if (src < 0) continue;
     float acc = 0.0f;
     for (int t = 0; t < nt; ++t) {
@@ -108,43 +114,88 @@ struct DevTb {
   int64_t bits_out;  // offset of the block's TBS output bits
 };
 
-// One warp per transport block (lte_turbo.cpp:958-979): hard decisions (>= 0 -> 1), the first
-// code block's filler dropped, CRC24B checked and stripped when C > 1, blocks concatenated, and
-// CRC24A checked over TBS + 24 bits.  A CRC is a syndrome: the XOR of x^(N-1-j) mod g over the
-// set bits j of the N-bit codeword.
-__global__ void tb_finish_kernel(const DevTb* __restrict__ tbs, int n_tb, const DevCb* __restrict__ cbs,
-                                 const float* __restrict__ post, const uint32_t* __restrict__ xpow_a,
-                                 const uint32_t* __restrict__ xpow_b, uint8_t* __restrict__ bits,
-                                 uint8_t* __restrict__ tb_ok, uint8_t* __restrict__ cb_ok) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= n_tb) return;
-  const DevTb t = tbs[warp];
-  const int64_t n_a = t.tbs + 24;  // TB codeword length with CRC24A
-  uint32_t syn_a = 0;
-  int64_t pos = 0;  // bit position in the TB + CRC24A stream
-  for (int r = 0; r < t.n_cb; ++r) {
-    const DevCb cb = cbs[t.first_cb + r];
-    const int n_b = cb.k - cb.filler;                        // CRC24B codeword length
-    const int keep = n_b - (t.n_cb > 1 ? 24 : 0);            // bits that join the TB stream
-    uint32_t syn_b = 0;
-    for (int i = lane; i < n_b; i += 32) {
-      const uint8_t bit = post[cb.out + cb.filler + i] >= 0.0f ? 1 : 0;
-      if (bit) syn_b ^= xpow_b[n_b - 1 - i];
-      if (i < keep) {
-        const int64_t j = pos + i;
-        if (bit && j < n_a) syn_a ^= xpow_a[n_a - 1 - j];
-        if (j < t.tbs) bits[t.bits_out + j] = bit;
-      }
+// Per code block of a transport-block call: its transport block and where its kept bits start in
+// that block's TBS + CRC24A stream (the sum of the kept bits of the blocks before it).
+struct DevTbCb {
+  int32_t tb;
+  int32_t pos;
+};
+
+constexpr int kFinishThreads = 256;
+
+// Finish, part 1 (lte_turbo.cpp:958-979), one CTA per code block: hard decisions (>= 0 -> 1)
+// of bits [filler, K), the CRC24B syndrome over them (checked when C > 1), the kept bits (the
+// CRC24B dropped when C > 1) written at their place in the transport block's output, and this
+// block's share of the transport block's CRC24A syndrome.  A CRC is a syndrome: the XOR of
+// x^(N-1-j) mod g over the set bits j of the N-bit codeword, so the shares of a transport
+// block's code blocks XOR to its syndrome.
+__global__ void __launch_bounds__(kFinishThreads) tb_finish_cb_kernel(
+    const DevTb* __restrict__ tbs, const DevTbCb* __restrict__ tbcb, const DevCb* __restrict__ cbs,
+    const float* __restrict__ post, const uint32_t* __restrict__ xpow_a,
+    const uint32_t* __restrict__ xpow_b, uint8_t* __restrict__ bits, uint8_t* __restrict__ cb_ok,
+    uint32_t* __restrict__ syn_a_part) {
+  __shared__ uint32_t red[2][kFinishThreads / 32];
+  const int c = blockIdx.x;
+  const DevTbCb m = tbcb[c];
+  if (m.tb < 0) {  // in no transport block
+    if (threadIdx.x == 0) {
+      cb_ok[c] = 0;
+      syn_a_part[c] = 0;
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) syn_b ^= __shfl_xor_sync(0xffffffffu, syn_b, o);
-    if (lane == 0) cb_ok[t.first_cb + r] = (t.n_cb == 1) ? 1 : (syn_b == 0);
-    pos += keep;
+    return;
+  }
+  const DevTb t = tbs[m.tb];
+  const DevCb cb = cbs[c];
+  const int64_t n_a = t.tbs + 24;             // TB codeword length with CRC24A
+  const int n_b = cb.k - cb.filler;           // CRC24B codeword length
+  const int keep = n_b - (t.n_cb > 1 ? 24 : 0);
+  uint32_t syn_b = 0, syn_a = 0;
+  for (int i = threadIdx.x; i < n_b; i += kFinishThreads) {
+    const uint8_t bit = post[cb.out + cb.filler + i] >= 0.0f ? 1 : 0;
+    if (bit) syn_b ^= xpow_b[n_b - 1 - i];
+    if (i < keep) {
+      const int64_t j = m.pos + i;
+      if (bit && j < n_a) syn_a ^= xpow_a[n_a - 1 - j];
+      if (j < t.tbs) bits[t.bits_out + j] = bit;
+    }
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) syn_a ^= __shfl_xor_sync(0xffffffffu, syn_a, o);
-  if (lane == 0) tb_ok[warp] = (pos == n_a) && syn_a == 0;
+  for (int o = 16; o > 0; o >>= 1) {
+    syn_b ^= __shfl_xor_sync(0xffffffffu, syn_b, o);
+    syn_a ^= __shfl_xor_sync(0xffffffffu, syn_a, o);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[0][wid] = syn_b;
+    red[1][wid] = syn_a;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t b = 0, a = 0;
+    for (int w = 0; w < kFinishThreads / 32; ++w) {
+      b ^= red[0][w];
+      a ^= red[1][w];
+    }
+    cb_ok[c] = (t.n_cb == 1) ? 1 : (b == 0);
+    syn_a_part[c] = a;
+  }
+}
+
+// Finish, part 2, one thread per transport block: the XOR of its code blocks' CRC24A shares,
+// and whether the kept bits add up to TBS + 24.
+__global__ void tb_finish_tb_kernel(const DevTb* __restrict__ tbs, int n_tb,
+                                    const DevTbCb* __restrict__ tbcb, const DevCb* __restrict__ cbs,
+                                    const uint32_t* __restrict__ syn_a_part,
+                                    uint8_t* __restrict__ tb_ok) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_tb) return;
+  const DevTb d = tbs[t];
+  uint32_t a = 0;
+  for (int r = 0; r < d.n_cb; ++r) a ^= syn_a_part[d.first_cb + r];
+  const int last = d.first_cb + d.n_cb - 1;
+  const DevCb cb = cbs[last];
+  const int64_t kept_end = tbcb[last].pos + cb.k - cb.filler - (d.n_cb > 1 ? 24 : 0);
+  tb_ok[t] = (kept_end == d.tbs + 24) && a == 0;
 }
 
 std::vector<uint32_t> xpow_table(CrcKind kind, size_t n, Convention conv) {
@@ -296,6 +347,20 @@ void Decoder::transport_blocks(const TbRequest& q, bool wait, void* after, void*
     tbs[t] = DevTb{d.first_cb, d.n_cb, d.tbs, d.bits_offset};
     bits_len = std::max<int64_t>(bits_len, d.bits_offset + d.tbs);
   }
+  // per code block: its transport block and the start of its kept bits in that block's stream
+  // (a block that belongs to no transport block keeps tb = -1: decoded, then left out)
+  std::vector<DevTbCb> tbcb(q.n_cb, DevTbCb{-1, 0});
+  for (size_t t = 0; t < q.n_tb; ++t) {
+    int64_t pos = 0;
+    for (int r = 0; r < tbs[t].n_cb; ++r) {
+      const auto& c = q.cbs[tbs[t].first_cb + r];
+      if (tbcb[tbs[t].first_cb + r].tb >= 0)
+        throw InvalidArgument("a code block belongs to two transport blocks");
+      tbcb[tbs[t].first_cb + r] = DevTbCb{static_cast<int32_t>(t), static_cast<int32_t>(pos)};
+      pos += c.k - c.filler - (tbs[t].n_cb > 1 ? 24 : 0);
+    }
+  }
+
   if (q.n_tb == 0) return;
   // ---- device buffers ----
   const float* e_llr = q.e_llr;
@@ -314,6 +379,8 @@ void Decoder::transport_blocks(const TbRequest& q, bool wait, void* after, void*
   uint32_t* iters = q.device_memory && q.iterations_used ? q.iterations_used
                                                          : grow<uint32_t>(d_tbiters_, q.n_cb);
   DevTb* dtb = grow<DevTb>(d_tb_, q.n_tb);
+  DevTbCb* dtbcb = grow<DevTbCb>(d_tbcb_, q.n_cb);
+  uint32_t* dsyn = grow<uint32_t>(d_synpart_, q.n_cb);
   const bool std3gpp = q.decode.std3gpp;
   DeviceBuffer& xpow_a = std3gpp ? d_xpow_a_std_ : d_xpow_a_;  // x^j mod g_CRC24A
   if (xpow_a.bytes == 0) {
@@ -344,12 +411,15 @@ void Decoder::transport_blocks(const TbRequest& q, bool wait, void* after, void*
     if (rq.persistent) decode_persistent(rq); else decode_plain(rq);
     // decode_* chained its own completion event; the finish kernel follows on the same stream
     upload(dtb, tbs.data(), q.n_tb * sizeof(DevTb), st);
-    tb_finish_kernel<<<static_cast<unsigned>((q.n_tb * 32 + 255) / 256), 256, 0, st>>>(
-        dtb, static_cast<int>(q.n_tb), static_cast<const DevCb*>(d_cbs_.ptr), post,
-        static_cast<const uint32_t*>(xpow_a.ptr),
-        static_cast<const uint32_t*>(std3gpp ? d_xpow_std_.ptr : d_xpow_.ptr), bits, tb_ok, cb_ok);
+    upload(dtbcb, tbcb.data(), q.n_cb * sizeof(DevTbCb), st);
+    const DevCb* dcbs = static_cast<const DevCb*>(d_cbs_.ptr);
+    tb_finish_cb_kernel<<<static_cast<unsigned>(q.n_cb), kFinishThreads, 0, st>>>(
+        dtb, dtbcb, dcbs, post, static_cast<const uint32_t*>(xpow_a.ptr),
+        static_cast<const uint32_t*>(std3gpp ? d_xpow_std_.ptr : d_xpow_.ptr), bits, cb_ok, dsyn);
+    tb_finish_tb_kernel<<<static_cast<unsigned>((q.n_tb + 255) / 256), 256, 0, st>>>(
+        dtb, static_cast<int>(q.n_tb), dtbcb, dcbs, dsyn, tb_ok);
     check(cudaGetLastError(), "finish launch");
-    timing_.launches += 1;
+    timing_.launches += 2;
     if (q.device_memory && q.posterior)
       check(cudaMemcpyAsync(q.posterior, post, static_cast<size_t>(post_len) * 4,
                             cudaMemcpyDeviceToDevice, st), "copy");

@@ -35,6 +35,51 @@ __device__ __forceinline__ int rm_source(int pos, int d, int rows, int kpi, int 
   return y < 0 ? -1 : 2 * d + y;  // parity 2: no filler nulling
 }
 
+// Sources of consecutive circular-buffer positions from p on, with the divisions by `rows` of
+// rm_source done once: the position's (or, in the parity part, its interlaced lane's) quotient
+// and remainder by `rows` are advanced incrementally.  next() returns the source of the current
+// position (as rm_source) and moves to the following one.
+struct CircularWalk {
+  int d, rows, kpi, dummy, filler;
+  int pos, q, r;  // systematic part: pos = q*rows + r; parity part: lane = q*rows + r
+
+  __device__ __forceinline__ CircularWalk(int p, int d_, int rows_, int kpi_, int filler_)
+      : d(d_), rows(rows_), kpi(kpi_), dummy(kpi_ - d_), filler(filler_), pos(p) {
+    const int idx = p < kpi ? p : (p - kpi) >> 1;
+    q = idx / rows;
+    r = idx - q * rows;
+  }
+
+  __device__ __forceinline__ int next() {
+    int src;
+    if (pos < kpi) {  // systematic, read column by column
+      const int y = r * 32 + c_col_perm[q] - dummy;
+      src = (y < 0 || y < filler) ? -1 : y;
+      if (++r == rows) {
+        r = 0;
+        ++q;
+      }
+      if (++pos == kpi) q = r = 0;  // the parity part starts at lane 0
+      return src;
+    }
+    if (((pos - kpi) & 1) == 0) {  // parity 1: same permutation as the systematic stream
+      const int y = r * 32 + c_col_perm[q] - dummy;
+      src = (y < 0 || y < filler) ? -1 : d + y;
+    } else {  // parity 2: no filler nulling; the lane advances after its second stream
+      int y = c_col_perm[q] + 32 * r + 1;
+      if (y >= kpi) y -= kpi;
+      y -= dummy;
+      src = y < 0 ? -1 : 2 * d + y;
+      if (++r == rows) {
+        r = 0;
+        ++q;
+      }
+    }
+    ++pos;
+    return src;
+  }
+};
+
 // The circular buffer of one code block as one CTA of kCircThreads threads sees it: each thread
 // owns the positions [p0, p1); `before` is the number of valid positions before p0.
 struct CircularScan {
@@ -61,11 +106,17 @@ struct CircularScan {
     return rows * (2 * ((ncb + 8 * rows - 1) / (8 * rows)) * rv + 2) % ncb;
   }
 
+  // the sources of positions p, p+1, ... in order
+  __device__ __forceinline__ CircularWalk walk(int p) const {
+    return CircularWalk(p, d, rows, kpi, filler);
+  }
+
   // Block-wide exclusive scan of the valid-position counts; every thread must call it.
   // warp_sum: kCircThreads / 32 ints of shared memory; s_total: one shared int.
   __device__ __forceinline__ void scan(int* warp_sum, int* s_total) {
     int cnt = 0;
-    for (int p = p0; p < p1; ++p) cnt += source(p) >= 0;
+    CircularWalk wk = walk(p0);
+    for (int p = p0; p < p1; ++p) cnt += wk.next() >= 0;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int incl = cnt;
 #pragma unroll
@@ -93,7 +144,8 @@ struct CircularScan {
   __device__ __forceinline__ void rank_of(int pos, int* out) const {
     if (pos >= p0 && pos < p1) {
       int r = before;
-      for (int p = p0; p < pos; ++p) r += source(p) >= 0;
+      CircularWalk wk = walk(p0);
+      for (int p = p0; p < pos; ++p) r += wk.next() >= 0;
       *out = r;
     }
   }

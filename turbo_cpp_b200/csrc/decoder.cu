@@ -181,7 +181,7 @@ Decoder::~Decoder() {
   for (DeviceBuffer* b : {&d_perm_, &d_inv_, &d_xpow_, &d_xpow_std_, &d_xpow_a_std_, &d_cbs_, &d_wincb_, &d_llr_,
                           &d_sysi_, &d_e1i_, &d_e2_, &d_post_, &d_seed_, &d_done_, &d_iters_,
                           &d_crc_, &d_ckpt_, &d_tasks_, &d_queue_, &d_rm_, &d_e_llr_, &d_d012_,
-                          &d_tbpost_, &d_tbbits_, &d_tbok_, &d_cbok_, &d_tbiters_, &d_tb_,
+                          &d_tbpost_, &d_tbbits_, &d_tbok_, &d_cbok_, &d_tbiters_, &d_tb_, &d_tbcb_, &d_synpart_,
                           &d_xpow_a_, &d_rmgroup_, &d_gen_, &d_gentab_, &d_genenc_, &d_genrm_})
     b->release();
 }

@@ -247,6 +247,7 @@ class Decoder {
   DeviceBuffer d_cbs_, d_wincb_, d_llr_, d_sysi_, d_e1i_, d_e2_, d_post_, d_seed_,
       d_done_, d_iters_, d_crc_, d_ckpt_, d_tasks_, d_queue_;
   DeviceBuffer d_rmgroup_, d_gen_, d_gentab_, d_genenc_, d_genrm_, d_xpow_a_std_;
+  DeviceBuffer d_tbcb_, d_synpart_;
   DeviceBuffer d_rm_, d_e_llr_, d_d012_, d_tbpost_, d_tbbits_, d_tbok_, d_cbok_, d_tbiters_, d_tb_,
       d_xpow_a_;
   int persist_blocks_per_sm_ = 0;

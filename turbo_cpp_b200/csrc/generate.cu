@@ -182,8 +182,9 @@ __global__ void __launch_bounds__(kRmGenThreads) rate_match_kernel(const RmGen* 
   const uint8_t* src_bits = d012 + b.d_off;
   uint8_t* out = e_bits + b.e_off;
   int rank = cs.before;
+  CircularWalk wk = cs.walk(cs.p0);
   for (int p = cs.p0; p < cs.p1; ++p) {
-    const int src = cs.source(p);
+    const int src = wk.next();
     if (src < 0) continue;
     int kk = rank - r0;
     if (kk < 0) kk += nv;
