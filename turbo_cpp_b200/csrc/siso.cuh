@@ -20,6 +20,10 @@
 
 #include "trellis.cuh"
 
+#ifndef TCB_LDCG
+#define TCB_LDCG 0
+#endif
+
 namespace tcb {
 
 // Per-code-block descriptor as the kernels see it (built by the host decoder).
@@ -57,12 +61,16 @@ __device__ __forceinline__ float4 ld4(const float* p) {
 // releases and the reader acquires at GPU scope before these loads, which makes them see the
 // writes even when the writer ran on another SM.
 __device__ __forceinline__ float4 ld4_coherent(const float* p) {
+#if TCB_LDCG
+  return __ldcg(reinterpret_cast<const float4*>(p));
+#else
   float4 v;
   asm volatile("ld.global.v4.f32 {%0, %1, %2, %3}, [%4];"
                : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
                : "l"(p)
                : "memory");
   return v;
+#endif
 }
 template <bool COHERENT>
 __device__ __forceinline__ float4 ld4_io(const float* p) {
