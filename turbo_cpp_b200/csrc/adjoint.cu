@@ -21,10 +21,11 @@
 // difference of two log-sums over the same metrics, so they are constants of the function and
 // the adjoint ignores them.  A warm-up step of one window is an output step of its neighbour, so
 // each window writes its own steps' gradients and its warm-up gradients to separate arrays; a
-// combine kernel adds the three contributions of every position in a fixed order (the result is
-// deterministic), scatters them to d0/d1/d2 and to the other SISO's a-priori adjoint, and adds
-// the tail gradients.  d loss / d scale_j is the sum of d loss / d e * x over the SISO's
-// positions (x its unscaled extrinsic), reduced per window and then in a fixed order.
+// combine kernel (one CTA per code block) adds the three contributions of every position in a
+// fixed order (the result is deterministic), adds them to d0/d1/d2 and writes the other SISO's
+// a-priori adjoint, and adds the tail gradients.  d loss / d scale_j is the sum of
+// d loss / d e * x over the SISO's positions (x its unscaled extrinsic), reduced per window, per
+// code block and then over the blocks, each in a fixed order.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -466,84 +467,121 @@ struct CombineIo {
   const float* own_par;
   const float* guard_g;
   const float* tail_g;
-  const uint16_t* perm;
+  const uint16_t* inv;     // lower SISO: natural position q is SISO position inv[q]
   const float* grad_post;  // posterior layout
+  const float* win_part;   // [launch window]: this SISO's sum of ge * x per window
   float* grad_llr;         // LLR layout
   float* ge_out;           // upper: d/d e2 of the previous iteration; lower: d/d e1 (natural)
+  double* cb_part;         // [code block]: the block's windows' win_part, summed in window order
 };
 
-// Position p of code block cb in the SISO's order: own + neighbours' warm-up gradients, then
-// d0/d1/d2 and the adjoint of the a-priori (the other SISO's scaled extrinsic).
-template <bool LOWER, bool LAST, bool STD>
-__device__ __forceinline__ void combine_position(const CombineIo& c, const DevCb& cb, int p) {
-  const int W = cb.window, G = c.guard, K = cb.k;
+constexpr int kMaxK = 6144;  // largest QPP block size
+constexpr int kCombineThreads = 256;
+
+// d loss / d(Ls+La) and d loss / d Lp at SISO position p: its own window's gradient, then the
+// alpha warm-up gradient of window w+1, then the beta warm-up gradient of window w-1 (a fixed
+// order, so the result is deterministic).
+__device__ __forceinline__ void position_grads(const CombineIo& c, const DevCb& cb, int p,
+                                               float& sa, float& par) {
+  const int W = cb.window, G = c.guard;
   const int w = p / W, lo = w * W;
-  float sa = c.own_sa[cb.work + p], par = c.own_par[cb.work + p];
-  if (w + 1 < cb.nwin && p >= lo + W - G) {  // alpha warm-up of window w+1
+  sa = c.own_sa[cb.work + p];
+  par = c.own_par[cb.work + p];
+  if (w + 1 < cb.nwin && p >= lo + W - G) {
     const float* ag = c.guard_g + static_cast<int64_t>(4 * (cb.win0 + w + 1)) * G;
     const int j = p - (lo + W - G);
     sa += ag[j];
     par += ag[G + j];
   }
-  if (w > 0 && p < lo + G) {  // beta warm-up of window w-1
+  if (w > 0 && p < lo + G) {
     const float* bg = c.guard_g + static_cast<int64_t>(4 * (cb.win0 + w - 1)) * G + 2 * G;
     const int j = p - lo;
     sa += bg[j];
     par += bg[G + j];
   }
-  float* g0 = c.grad_llr + cb.llr;
+}
+
+// Tail LLRs: the tail-started windows' gradients summed in window order.
+template <bool LOWER, bool STD>
+__device__ __forceinline__ void combine_tail(const CombineIo& c, const DevCb& cb, float* g0) {
+  const int W = cb.window, G = c.guard, K = cb.k;
   float* g1 = g0 + (K + 4);
   float* g2 = g1 + (K + 4);
-  if (!LOWER) {
-    g0[p] += sa;
-    g1[p] += par;
-    c.ge_out[cb.work + p] = sa;
-  } else {
-    const int q = c.perm[cb.tab + p];
-    g0[q] += sa;
-    g2[p] += par;
-    c.ge_out[cb.work + q] = sa + (LAST ? c.grad_post[cb.out + q] : 0.0f);
+  float gt[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+  for (int v = 0; v < cb.nwin; ++v) {
+    if (min((v + 1) * W, K) + G < K) continue;
+    const float* t = c.tail_g + 8 * (cb.win0 + v);
+    for (int k = 0; k < 6; ++k) gt[k] += t[k];
   }
-  if (p == 0) {  // tail LLRs, summed over the tail-started windows in window order
-    float gt[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-    for (int v = 0; v < cb.nwin; ++v) {
-      if (min((v + 1) * W, K) + G < K) continue;
-      const float* t = c.tail_g + 8 * (cb.win0 + v);
-      for (int k = 0; k < 6; ++k) gt[k] += t[k];
-    }
-    if (STD) {  // 36.212: ts = {d0[K+o], d2[K+o], d1[K+o+1]}, tp = {d1[K+o], d0[K+o+1], d2[K+o+1]}
-      const int o = LOWER ? 2 : 0;
-      g0[K + o] += gt[0];
-      g2[K + o] += gt[1];
-      g1[K + o + 1] += gt[2];
-      g1[K + o] += gt[3];
-      g0[K + o + 1] += gt[4];
-      g2[K + o + 1] += gt[5];
-    } else if (!LOWER) {  // ts = {d0[K], d0[K+2], 0}, tp = {d1[K], d0[K+1], d1[K+2]}
-      g0[K] += gt[0];
-      g0[K + 2] += gt[1];
-      g1[K] += gt[3];
-      g0[K + 1] += gt[4];
-      g1[K + 2] += gt[5];
-    } else {  // ts = {d1[K+3], d2[K], d2[K+2]}, tp = {d2[K+1], d0[K+3], d2[K+3]}
-      g1[K + 3] += gt[0];
-      g2[K] += gt[1];
-      g2[K + 2] += gt[2];
-      g2[K + 1] += gt[3];
-      g0[K + 3] += gt[4];
-      g2[K + 3] += gt[5];
-    }
+  if (STD) {  // 36.212: ts = {d0[K+o], d2[K+o], d1[K+o+1]}, tp = {d1[K+o], d0[K+o+1], d2[K+o+1]}
+    const int o = LOWER ? 2 : 0;
+    g0[K + o] += gt[0];
+    g2[K + o] += gt[1];
+    g1[K + o + 1] += gt[2];
+    g1[K + o] += gt[3];
+    g0[K + o + 1] += gt[4];
+    g2[K + o + 1] += gt[5];
+  } else if (!LOWER) {  // ts = {d0[K], d0[K+2], 0}, tp = {d1[K], d0[K+1], d1[K+2]}
+    g0[K] += gt[0];
+    g0[K + 2] += gt[1];
+    g1[K] += gt[3];
+    g0[K + 1] += gt[4];
+    g1[K + 2] += gt[5];
+  } else {  // ts = {d1[K+3], d2[K], d2[K+2]}, tp = {d2[K+1], d0[K+3], d2[K+3]}
+    g1[K + 3] += gt[0];
+    g2[K] += gt[1];
+    g2[K + 2] += gt[2];
+    g2[K + 1] += gt[3];
+    g0[K + 3] += gt[4];
+    g2[K + 3] += gt[5];
   }
 }
 
-// One thread per position; as setup_kernel, the grid's y index walks the code blocks and its x
-// index (kSetupBlocksPerCb x kSetupThreads) the positions of one block.
+// One block per code block.  Adds the SISO's gradients to d0/d1 (upper, natural order) or to
+// d2 (lower, SISO order) and d0 (lower: staged in shared memory by SISO position, then gathered
+// through the inverse permutation so that every global access walks the natural order), writes
+// the adjoint of the a-priori (the other SISO's scaled extrinsic; plus d loss / d posterior for
+// the last lower SISO, whose extrinsic also enters the posterior), adds the tail gradients, and
+// sums the block's per-window scale parts in a fixed order.
 template <bool LOWER, bool LAST, bool STD = false>
-__global__ void adj_combine_kernel(CombineIo c) {
-  const int p = blockIdx.x * kSetupThreads + threadIdx.x;
-  for (int i = blockIdx.y; i < c.n_cb; i += gridDim.y) {
+__global__ void __launch_bounds__(kCombineThreads) adj_combine_kernel(CombineIo c) {
+  __shared__ float sa_s[LOWER ? kMaxK : 1];
+  __shared__ double red[kCombineThreads];
+  for (int i = blockIdx.x; i < c.n_cb; i += gridDim.x) {
     const DevCb cb = c.cbs[i];
-    if (p < cb.k) combine_position<LOWER, LAST, STD>(c, cb, p);
+    const int K = cb.k;
+    float* g0 = c.grad_llr + cb.llr;
+    for (int p = threadIdx.x; p < K; p += kCombineThreads) {
+      float sa, par;
+      position_grads(c, cb, p, sa, par);
+      if (!LOWER) {
+        g0[p] += sa;
+        g0[(K + 4) + p] += par;
+        c.ge_out[cb.work + p] = sa;
+      } else {
+        g0[2 * (K + 4) + p] += par;
+        sa_s[p] = sa;
+      }
+    }
+    if (threadIdx.x == 0) combine_tail<LOWER, STD>(c, cb, g0);
+    double s = 0.0;
+    for (int v = threadIdx.x; v < cb.nwin; v += kCombineThreads) s += c.win_part[cb.win0 + v];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    if (LOWER) {
+      const uint16_t* inv = c.inv + cb.tab;
+      for (int q = threadIdx.x; q < K; q += kCombineThreads) {
+        const float v = sa_s[inv[q]];
+        g0[q] += v;
+        c.ge_out[cb.work + q] = v + (LAST ? c.grad_post[cb.out + q] : 0.0f);
+      }
+    }
+    for (int o = kCombineThreads / 2; o > 0; o >>= 1) {
+      if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) c.cb_part[i] = red[0];
+    __syncthreads();  // sa_s and red are reused by the next code block
   }
 }
 
@@ -563,13 +601,13 @@ __global__ void adj_init_kernel(const DevCb* __restrict__ cbs, int n_cb,
   }
 }
 
-// grad_scales[j] = sum over windows of part[j][window], in a fixed order (one block per j).
-__global__ void adj_scale_reduce_kernel(const float* __restrict__ part, int n_win,
+// grad_scales[j] = sum over code blocks of cb_part[j][block], in a fixed order (one block per j).
+__global__ void adj_scale_reduce_kernel(const double* __restrict__ cb_part, int n_cb,
                                         float* __restrict__ grad_scales) {
   __shared__ double acc[256];
   const int j = blockIdx.x;
   double s = 0.0;
-  for (int i = threadIdx.x; i < n_win; i += blockDim.x) s += part[static_cast<int64_t>(j) * n_win + i];
+  for (int i = threadIdx.x; i < n_cb; i += blockDim.x) s += cb_part[static_cast<int64_t>(j) * n_cb + i];
   acc[threadIdx.x] = s;
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {
@@ -589,7 +627,7 @@ T* reserve(DeviceBuffer& b, size_t count) {
 
 Adjoint::~Adjoint() {
   for (DeviceBuffer* b : {&d_cbs_, &d_wincb_, &d_sysi_, &d_tape_, &d_seeds_, &d_ckpt_,
-                          &d_own_, &d_guard_, &d_tail_, &d_part_, &d_ge2_, &d_ga1_})
+                          &d_own_, &d_guard_, &d_tail_, &d_part_, &d_cbpart_, &d_ge2_, &d_ga1_})
     b->release();
 }
 
@@ -710,7 +748,8 @@ void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr
   float* own = reserve<float>(d_own_, 2 * static_cast<size_t>(work));
   float* guard_g = reserve<float>(d_guard_, static_cast<size_t>(n_win) * 4 * std::max(G, 4));
   float* tail_g = reserve<float>(d_tail_, static_cast<size_t>(n_win) * 8);
-  float* part = reserve<float>(d_part_, static_cast<size_t>(2 * I) * n_win);
+  float* part = reserve<float>(d_part_, static_cast<size_t>(n_win));
+  double* cb_part = reserve<double>(d_cbpart_, static_cast<size_t>(2 * I) * n_cb_);
   float* ge2 = reserve<float>(d_ge2_, work);
   float* ga1 = reserve<float>(d_ga1_, work);
   float4* ckpt = reserve<float4>(d_ckpt_, ckpt_slab(n_win, 4 * static_cast<size_t>(ckpt_bwd_)));
@@ -720,8 +759,10 @@ void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr
   const float* tape = static_cast<const float*>(d_tape_.ptr);
   const float* seeds = static_cast<const float*>(d_seeds_.ptr);
   const uint16_t* dperm = dec_.perm_table();
+  const uint16_t* dinv = dec_.inv_table();
   const int n = static_cast<int>(n_cb_);
   const dim3 pos_blocks(kSetupBlocksPerCb, static_cast<unsigned>(n < 65535 ? n : 65535));
+  const unsigned cb_blocks = static_cast<unsigned>(std::min(n, 1 << 20));
 
   ok(cudaMemsetAsync(grad_llr, 0, llr_len_ * sizeof(float), st), "zero grad_llr");
   adj_init_kernel<<<pos_blocks, kSetupThreads, 0, st>>>(dcbs, n, grad_post, grad_llr, ge2);
@@ -732,7 +773,7 @@ void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr
     const bool lower = j & 1;
     const bool last = j + 2 >= static_cast<int>(2 * I);  // a SISO of the last iteration
     AdjIo io{llr_, sysi, tape + j * work, lower ? ge2 : ga1, dperm, seeds + j * slab, own,
-             own + work, guard_g, tail_g, part + static_cast<int64_t>(j) * n_win, ckpt, ckpt_bwd_,
+             own + work, guard_g, tail_g, part, ckpt, ckpt_bwd_,
              scales_[j], G};
     if (std3gpp_) {
       if (lower) {
@@ -750,26 +791,26 @@ void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr
       siso_adjoint_kernel<false, 2><<<blocks, kAdjThreads, 0, st>>>(dcbs, dwin, n_win, io);
     }
     ok(cudaGetLastError(), "SISO adjoint launch");
-    CombineIo c{dcbs, n, G, own, own + work, guard_g, tail_g, dperm, grad_post, grad_llr,
-                lower ? ga1 : ge2};
+    CombineIo c{dcbs, n, G, own, own + work, guard_g, tail_g, dinv, grad_post, part, grad_llr,
+                lower ? ga1 : ge2, cb_part + static_cast<int64_t>(j) * n};
     if (std3gpp_) {
       if (lower && last)
-        adj_combine_kernel<true, true, true><<<pos_blocks, kSetupThreads, 0, st>>>(c);
+        adj_combine_kernel<true, true, true><<<cb_blocks, kCombineThreads, 0, st>>>(c);
       else if (lower)
-        adj_combine_kernel<true, false, true><<<pos_blocks, kSetupThreads, 0, st>>>(c);
+        adj_combine_kernel<true, false, true><<<cb_blocks, kCombineThreads, 0, st>>>(c);
       else
-        adj_combine_kernel<false, false, true><<<pos_blocks, kSetupThreads, 0, st>>>(c);
+        adj_combine_kernel<false, false, true><<<cb_blocks, kCombineThreads, 0, st>>>(c);
     } else if (lower && last) {
-      adj_combine_kernel<true, true><<<pos_blocks, kSetupThreads, 0, st>>>(c);
+      adj_combine_kernel<true, true><<<cb_blocks, kCombineThreads, 0, st>>>(c);
     } else if (lower) {
-      adj_combine_kernel<true, false><<<pos_blocks, kSetupThreads, 0, st>>>(c);
+      adj_combine_kernel<true, false><<<cb_blocks, kCombineThreads, 0, st>>>(c);
     } else {
-      adj_combine_kernel<false, false><<<pos_blocks, kSetupThreads, 0, st>>>(c);
+      adj_combine_kernel<false, false><<<cb_blocks, kCombineThreads, 0, st>>>(c);
     }
     ok(cudaGetLastError(), "adjoint combine launch");
     launches_ += 3;
   }
-  adj_scale_reduce_kernel<<<2 * I, 256, 0, st>>>(part, n_win, grad_scales);
+  adj_scale_reduce_kernel<<<2 * I, 256, 0, st>>>(cb_part, n, grad_scales);
   ok(cudaGetLastError(), "scale reduce launch");
   launches_ += 1;
 }

@@ -68,7 +68,7 @@ class Adjoint {
   std::vector<float> scales_;
   const float* llr_ = nullptr;
   DeviceBuffer d_cbs_, d_wincb_, d_sysi_, d_tape_, d_seeds_, d_ckpt_;
-  DeviceBuffer d_own_, d_guard_, d_tail_, d_part_, d_ge2_, d_ga1_;
+  DeviceBuffer d_own_, d_guard_, d_tail_, d_part_, d_cbpart_, d_ge2_, d_ga1_;
 };
 
 }  // namespace tcb
