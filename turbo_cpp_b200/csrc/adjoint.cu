@@ -2,13 +2,13 @@
 //
 // Forward (taped): the plain decoder's SISO kernel, one launch per half-iteration, with the
 // a-priori input and extrinsic output of every half-iteration kept in its own tape slot (slot j
-// is SISO j's a-priori, slot j+1 its scaled extrinsic; slot 0 is zero) and the seeds of every
-// half-iteration in their own slab (SISO j reads slab j and writes slab j+2).
+// is SISO j's a-priori, slot j+1 its scaled extrinsic; slot 0 is zero), the seeds of every
+// half-iteration in their own slab (SISO j reads slab j and writes slab j+2), and the alpha
+// checkpoints of every half-iteration in their own slab: every 4 steps from the window's alpha
+// start (seed or block start) to its end, as log values.
 //
 // Backward: per half-iteration, last to first, one thread per window of the forward schedule
-// runs the adjoint of its window in three phases (base-2 metrics, as the forward):
-//   A  alpha from the window's forward start (seed or block start) to its end, a checkpoint
-//      every 4 steps;
+// runs the adjoint of its window in two phases (base-2 metrics, as the forward):
 //   B  backward in time from the beta start (seed or tail) to the alpha start: beta, stored
 //      every 4 steps; alpha recomputed from its checkpoint 4 steps at a time; the extrinsic's
 //      softmax weights give the direct alpha adjoint and d/d parity; the alpha adjoint
@@ -173,12 +173,16 @@ struct AdjIo {
   const float* ge;        // d loss / d (scaled extrinsic of this SISO), work layout, natural order
   const uint16_t* perm;   // lower SISO: position i's extrinsic is e2[perm[i]]
   const float* seeds;     // [launch window][16]: the seeds this SISO used
-  float* own_sa;          // [work]: d loss / d(Ls+La) of the window's own steps (SISO order)
-  float* own_par;         // [work]: d loss / d Lp
+  float4* alpha_ckpt;     // the taped alpha checkpoints of this SISO: ckpt_slots planes of n_win
+                          // float4 pairs, plane m = alpha at a_lo + 4m
+  float* own_sa;          // [work]: d loss / d(Ls+La) of the window's own steps (SISO order),
+                          // phase B's part; phase C's part follows at own_sa + 2 * work
+  float* own_par;         // [work]: d loss / d Lp (likewise)
+  int64_t work;
   float* guard_g;         // [launch window][4][guard]: alpha warm-up sa, par; beta warm-up sa, par
   float* tail_g;          // [launch window][8]: d/d ts[0..2], d/d tp[0..2] (tail-started windows)
   float* scale_part;      // [launch window]: sum of ge * x over the window
-  float4* ckpt;           // alpha then beta checkpoints: 2 * ckpt_slots planes of n_win float4 each
+  float4* ckpt;           // beta checkpoints: ckpt_slots planes of n_win float4 pairs
   int ckpt_slots;         // checkpoints of each kind per window
   float scale;
   int guard;
@@ -204,10 +208,9 @@ __device__ __forceinline__ void load_ge(const AdjIo& io, const DevCb& cb, bool l
   }
 }
 
-// PHASES: 1 = A and B, 2 = C, as separate launches (C reads what A and B stored in global
-// memory): each holds less live state, so that 6 blocks per SM (168 registers, at most 48 B
-// spilled) fit where the single kernel held 4 (234 registers); measured 8.63 against 8.94 ms
-// for the 12 backward half-iterations of 1024 blocks of K=6144.
+// PHASES: 1 = B, 2 = C, as separate launches (C reads what B stored in global memory): each
+// holds less live state, so that 6 blocks per SM (168 registers) fit where a single kernel held
+// 4 (234 registers).
 constexpr int kAdjMinBlocks = 6;
 template <bool LOWER, int PHASES, bool STD = false>
 __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kernel(const DevCb* __restrict__ cbs,
@@ -227,34 +230,15 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
   const float* sys = LOWER ? io.sys_i + cb.work : d0;
   const float* par = d0 + (LOWER ? 2 : 1) * (K + 4);
   const float* apr = io.apr + cb.work;
-  // alpha then beta checkpoints, each a slab of planes with the launch's windows interleaved
-  const CkptStrided cka{io.ckpt, n_win, g};
-  const CkptStrided ckb{io.ckpt + static_cast<int64_t>(2) * io.ckpt_slots * n_win, n_win, g};
+  // alpha (taped) and beta checkpoints, each a slab of planes with the launch's windows
+  // interleaved
+  const CkptStrided cka{io.alpha_ckpt, n_win, g};
+  const CkptStrided ckb{io.ckpt, n_win, g};
   float sa[4], a[4], b[4];
   float* ag = io.guard_g + static_cast<int64_t>(4 * g) * G;
   const float xs = kLn2 * io.scale;  // d e / d(base-2 extrinsic)
 
   if (PHASES & 1) {
-  // ---- A: alpha checkpoints (log values) at a_lo + 4m; the recursion itself runs in the
-  // deferred-log (m, s) form of the forward decoder (one ex2 per max*) ----
-  float al[8], as[8];
-  ms_ones(as);
-  if (start) alpha_start(al); else load8(io.seeds + 16 * g, al);
-  for (int q = a_lo; q < hi; q += 4) {
-    float v[8];
-    ms_to_log(al, as, v);
-    cka.store((q - a_lo) >> 2, v);
-    scale4(load_raw4(sys, apr, par, q), sa, a, b);
-#pragma unroll
-    for (int t = 0; t < 4; ++t) alpha_step_ms<STD>(al, as, a[t], b[t]);
-    ms_renorm(al, as);
-  }
-  if (!STD) {  // alpha at hi: the alpha_{t+1} of the window's last step (destination form)
-    float v[8];
-    ms_to_log(al, as, v);
-    cka.store((hi - a_lo) >> 2, v);
-  }
-
   // ---- B: backward in time ----
   float be[8];
   if (tail) {
@@ -427,11 +411,8 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
     }
     ms_renorm(al, as);
     if (own) {
-      float4* ps = reinterpret_cast<float4*>(io.own_sa + cb.work + P);
-      float4* pp = reinterpret_cast<float4*>(io.own_par + cb.work + P);
-      const float4 s4 = *ps, p4 = *pp;
-      *ps = make_float4(s4.x + gsa[0], s4.y + gsa[1], s4.z + gsa[2], s4.w + gsa[3]);
-      *pp = make_float4(p4.x + gpar[0], p4.y + gpar[1], p4.z + gpar[2], p4.w + gpar[3]);
+      *reinterpret_cast<float4*>(io.own_sa + 2 * io.work + cb.work + P) = make_float4(gsa[0], gsa[1], gsa[2], gsa[3]);
+      *reinterpret_cast<float4*>(io.own_par + 2 * io.work + cb.work + P) = make_float4(gpar[0], gpar[1], gpar[2], gpar[3]);
     } else {
       const int j = P - hi;
       *reinterpret_cast<float4*>(bg + j) = make_float4(gsa[0], gsa[1], gsa[2], gsa[3]);
@@ -463,8 +444,9 @@ struct CombineIo {
   const DevCb* cbs;
   int n_cb;
   int guard;
-  const float* own_sa;
+  const float* own_sa;     // phase B's own-step gradients; phase C's at + 2 * work
   const float* own_par;
+  int64_t work;
   const float* guard_g;
   const float* tail_g;
   const uint16_t* inv;     // lower SISO: natural position q is SISO position inv[q]
@@ -485,8 +467,8 @@ __device__ __forceinline__ void position_grads(const CombineIo& c, const DevCb& 
                                                float& sa, float& par) {
   const int W = cb.window, G = c.guard;
   const int w = p / W, lo = w * W;
-  sa = c.own_sa[cb.work + p];
-  par = c.own_par[cb.work + p];
+  sa = c.own_sa[cb.work + p] + c.own_sa[2 * c.work + cb.work + p];
+  par = c.own_par[cb.work + p] + c.own_par[2 * c.work + cb.work + p];
   if (w + 1 < cb.nwin && p >= lo + W - G) {
     const float* ag = c.guard_g + static_cast<int64_t>(4 * (cb.win0 + w + 1)) * G;
     const int j = p - (lo + W - G);
@@ -626,7 +608,7 @@ T* reserve(DeviceBuffer& b, size_t count) {
 }  // namespace
 
 Adjoint::~Adjoint() {
-  for (DeviceBuffer* b : {&d_cbs_, &d_wincb_, &d_sysi_, &d_tape_, &d_seeds_, &d_ckpt_,
+  for (DeviceBuffer* b : {&d_cbs_, &d_wincb_, &d_sysi_, &d_tape_, &d_seeds_, &d_tapeckpt_, &d_ckpt_,
                           &d_own_, &d_guard_, &d_tail_, &d_part_, &d_cbpart_, &d_ge2_, &d_ga1_})
     b->release();
 }
@@ -687,7 +669,6 @@ uint64_t Adjoint::forward(const AdjointRequest& rq) {
   std3gpp_ = rq.std3gpp;
   scales_.assign(2 * I, 1.0f);
   if (rq.scales) std::copy(rq.scales, rq.scales + 2 * I, scales_.begin());
-  ckpt_fwd_ = max_window / kSub + 1;
   ckpt_bwd_ = (max_window + guard) / 4 + 1;
 
   DevCb* dcbs = reserve<DevCb>(d_cbs_, n);
@@ -696,7 +677,9 @@ uint64_t Adjoint::forward(const AdjointRequest& rq) {
   float* tape = reserve<float>(d_tape_, static_cast<size_t>(2 * I + 1) * work);
   const size_t slab = static_cast<size_t>(n_win) * 16;
   float* seeds = reserve<float>(d_seeds_, (2 * I + 2) * slab);
-  float4* ckpt = reserve<float4>(d_ckpt_, ckpt_slab(n_win, 2 * static_cast<size_t>(ckpt_fwd_)));
+  // alpha checkpoints of every half-iteration, a slab each
+  const size_t aslab = ckpt_slab(n_win, 2 * static_cast<size_t>(ckpt_bwd_));
+  float4* actp = reserve<float4>(d_tapeckpt_, 2 * I * aslab);
   ok(cudaMemcpyAsync(dcbs, cbs_.data(), n * sizeof(DevCb), cudaMemcpyHostToDevice, st), "copy descriptors");
   ok(cudaMemcpyAsync(dwin, wincb.data(), n_win * sizeof(int32_t), cudaMemcpyHostToDevice, st), "copy descriptors");
   ok(cudaMemsetAsync(seeds, 0, 2 * slab * sizeof(float), st), "zero seeds");
@@ -712,20 +695,21 @@ uint64_t Adjoint::forward(const AdjointRequest& rq) {
     SisoIo io{rq.llr, sysi, tape + j * work, tape + (j + 1) * work,
               (j + 1 == 2 * I) ? rq.posterior : nullptr, dperm, dinv, seeds + j * slab,
               seeds + (j + 2) * slab, scales_[j], guard};
+    float4* ck = actp + j * aslab;
     if (rq.std3gpp) {
       if (!lower)
-        siso_plain_kernel<kSub, 0, true, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
+        siso_plain_kernel<kSub, 0, true, true, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ck, ckpt_bwd_);
       else if (j + 1 < 2 * I)
-        siso_plain_kernel<kSub, 1, true, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
+        siso_plain_kernel<kSub, 1, true, true, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ck, ckpt_bwd_);
       else
-        siso_plain_kernel<kSub, 2, true, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
+        siso_plain_kernel<kSub, 2, true, true, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ck, ckpt_bwd_);
     } else {
       if (!lower)
-        siso_plain_kernel<kSub, 0, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
+        siso_plain_kernel<kSub, 0, true, false, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ck, ckpt_bwd_);
       else if (j + 1 < 2 * I)
-        siso_plain_kernel<kSub, 1, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
+        siso_plain_kernel<kSub, 1, true, false, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ck, ckpt_bwd_);
       else
-        siso_plain_kernel<kSub, 2, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ckpt, ckpt_fwd_);
+        siso_plain_kernel<kSub, 2, true, false, true><<<blocks, kThreads, 0, st>>>(dcbs, dwin, n_win, io, nullptr, ck, ckpt_bwd_);
     }
     ok(cudaGetLastError(), "SISO launch");
     launches_ += 1;
@@ -745,14 +729,16 @@ void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr
   const int n_win = n_win_, G = guard_;
   const uint32_t I = iterations_;
   const size_t slab = static_cast<size_t>(n_win) * 16;
-  float* own = reserve<float>(d_own_, 2 * static_cast<size_t>(work));
+  float* own = reserve<float>(d_own_, 4 * static_cast<size_t>(work));
   float* guard_g = reserve<float>(d_guard_, static_cast<size_t>(n_win) * 4 * std::max(G, 4));
   float* tail_g = reserve<float>(d_tail_, static_cast<size_t>(n_win) * 8);
   float* part = reserve<float>(d_part_, static_cast<size_t>(n_win));
   double* cb_part = reserve<double>(d_cbpart_, static_cast<size_t>(2 * I) * n_cb_);
   float* ge2 = reserve<float>(d_ge2_, work);
   float* ga1 = reserve<float>(d_ga1_, work);
-  float4* ckpt = reserve<float4>(d_ckpt_, ckpt_slab(n_win, 4 * static_cast<size_t>(ckpt_bwd_)));
+  float4* ckpt = reserve<float4>(d_ckpt_, ckpt_slab(n_win, 2 * static_cast<size_t>(ckpt_bwd_)));
+  const size_t aslab = ckpt_slab(n_win, 2 * static_cast<size_t>(ckpt_bwd_));
+  float4* actp = static_cast<float4*>(d_tapeckpt_.ptr);
   const DevCb* dcbs = static_cast<const DevCb*>(d_cbs_.ptr);
   const int32_t* dwin = static_cast<const int32_t*>(d_wincb_.ptr);
   const float* sysi = static_cast<const float*>(d_sysi_.ptr);
@@ -772,8 +758,9 @@ void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr
   for (int j = static_cast<int>(2 * I) - 1; j >= 0; --j) {
     const bool lower = j & 1;
     const bool last = j + 2 >= static_cast<int>(2 * I);  // a SISO of the last iteration
-    AdjIo io{llr_, sysi, tape + j * work, lower ? ge2 : ga1, dperm, seeds + j * slab, own,
-             own + work, guard_g, tail_g, part, ckpt, ckpt_bwd_,
+    AdjIo io{llr_, sysi, tape + j * work, lower ? ge2 : ga1, dperm, seeds + j * slab,
+             actp + j * aslab, own,
+             own + work, work, guard_g, tail_g, part, ckpt, ckpt_bwd_,
              scales_[j], G};
     if (std3gpp_) {
       if (lower) {
@@ -791,7 +778,7 @@ void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr
       siso_adjoint_kernel<false, 2><<<blocks, kAdjThreads, 0, st>>>(dcbs, dwin, n_win, io);
     }
     ok(cudaGetLastError(), "SISO adjoint launch");
-    CombineIo c{dcbs, n, G, own, own + work, guard_g, tail_g, dinv, grad_post, part, grad_llr,
+    CombineIo c{dcbs, n, G, own, own + work, work, guard_g, tail_g, dinv, grad_post, part, grad_llr,
                 lower ? ga1 : ge2, cb_part + static_cast<int64_t>(j) * n};
     if (std3gpp_) {
       if (lower && last)

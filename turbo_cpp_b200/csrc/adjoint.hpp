@@ -62,12 +62,12 @@ class Adjoint {
   // layout of the taped forward pass
   size_t n_cb_ = 0, llr_len_ = 0, post_len_ = 0;
   int64_t work_ = 0;
-  int n_win_ = 0, guard_ = 0, ckpt_fwd_ = 0, ckpt_bwd_ = 0;
+  int n_win_ = 0, guard_ = 0, ckpt_bwd_ = 0;
   uint32_t iterations_ = 0;
   bool std3gpp_ = false;
   std::vector<float> scales_;
   const float* llr_ = nullptr;
-  DeviceBuffer d_cbs_, d_wincb_, d_sysi_, d_tape_, d_seeds_, d_ckpt_;
+  DeviceBuffer d_cbs_, d_wincb_, d_sysi_, d_tape_, d_seeds_, d_tapeckpt_, d_ckpt_;
   DeviceBuffer d_own_, d_guard_, d_tail_, d_part_, d_cbpart_, d_ge2_, d_ga1_;
 };
 

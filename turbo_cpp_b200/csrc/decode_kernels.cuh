@@ -17,8 +17,10 @@ constexpr int kThreads = 64;  // threads (windows) per block of the plain SISO k
 constexpr int kMinBlocks = 8;  // 16 warps per SM: at most 128 registers per thread
 
 // KIND: 0 = upper SISO, 1 = lower SISO, 2 = lower SISO that also writes the posterior;
-// STD: the TS 36.212 code instead of the reference's
-template <int S, int KIND, bool GLOBAL_CKPT, bool STD = false>
+// STD: the TS 36.212 code instead of the reference's; TAPE (with GLOBAL_CKPT): the alpha
+// checkpoints cover the warm-up too, plane (q - a_lo) / S of the slab for step q, and stay for
+// the adjoint (a slab of (window + guard) / S + 1 planes)
+template <int S, int KIND, bool GLOBAL_CKPT, bool STD = false, bool TAPE = false>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) siso_plain_kernel(const DevCb* __restrict__ cbs,
                                                               const int32_t* __restrict__ win_cb,
                                                               int n_win, SisoIo io,
@@ -35,7 +37,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) siso_plain_kernel(const 
   if (GLOBAL_CKPT) {
     // checkpoint slab: ckpt_per_thread planes of n_win float4 pairs (windows interleaved)
     CkptStrided ck{ckpt_global, n_win, g};
-    siso_window<S, KIND != 0, KIND == 2, CkptStrided, false, STD>(cb, w, g, io, ck);
+    if (TAPE) {  // plane 0 is alpha at a_lo
+      const int lo = w * cb.window;
+      ck.p += static_cast<int64_t>(2 * (min(lo, io.guard) / S)) * n_win;
+    }
+    siso_window<S, KIND != 0, KIND == 2, CkptStrided, false, STD, TAPE>(cb, w, g, io, ck);
   } else {
     CkptSmem ck{smem_ckpt, static_cast<int>(blockDim.x), static_cast<int>(threadIdx.x)};
     siso_window<S, KIND != 0, KIND == 2, CkptSmem, false, STD>(cb, w, g, io, ck);

@@ -184,8 +184,11 @@ constexpr float kDestMaxA = 1024.0f;
 // Ls + e1 + e2 (last iteration, early stop).  Both may be compile-time constants (the plain
 // kernels, one specialisation each) or run-time values (the persistent kernel, which keeps a
 // single copy of this code for both halves).  COHERENT: a-priori and seeds were written earlier
-// in the same kernel (persistent schedule).
-template <int S, class Ckpt, bool COHERENT, bool STD = false, bool SMALL_LOOPS = false>
+// in the same kernel (persistent schedule).  TAPE: the alpha warm-up steps also leave
+// checkpoints, at negative indexes (q - lo) / S (the caller's checkpoint store is offset by the
+// warm-up), so that [a_lo, hi] is covered every S steps for the adjoint.
+template <int S, class Ckpt, bool COHERENT, bool STD = false, bool SMALL_LOOPS = false,
+          bool TAPE = false>
 __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, const SisoIo& io,
                                                const Ckpt& ck, const bool LOWER, const bool POST) {
   static_assert(S == 4, "sub-windows are one float4 group of 4 steps");
@@ -216,7 +219,7 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
     for (int q = a_lo; q < hi; q += 4) {
       Raw4 nxt = cur;
       if (q + 4 < hi) nxt = load_raw4<COHERENT>(sys, apr, par, q + 4);
-      if (q >= lo) {
+      if (TAPE || q >= lo) {
         float v[8];
         ms_to_log(al, as, v);
         ck.store((q - lo) / S, v);
@@ -234,7 +237,7 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
       Raw8 nxt = cur;
       if (q + 8 < hi) nxt = load_raw8<COHERENT>(sys, apr, par, q + 8);
       float v[8];
-      if (q >= lo) {
+      if (TAPE || q >= lo) {
         ms_to_log(al, as, v);
         ck.store((q - lo) / S, v);
       }
@@ -242,7 +245,7 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
       amax = fmaxf(amax, fmaxf(fmaxf(fabsf(a[0]), fabsf(a[1])), fmaxf(fabsf(a[2]), fabsf(a[3]))));
 #pragma unroll
       for (int t = 0; t < 4; ++t) alpha_step_ms<STD>(al, as, a[t], b[t]);
-      if (q >= lo) {
+      if (TAPE || q >= lo) {
         ms_to_log(al, as, v);
         ck.store((q - lo) / S + 1, v);
       }
@@ -406,10 +409,11 @@ __device__ __forceinline__ void siso_window_rt(const DevCb& cb, int w, int g, co
     backward(std::false_type{});
 }
 
-template <int S, bool LOWER, bool POST, class Ckpt, bool COHERENT = false, bool STD = false>
+template <int S, bool LOWER, bool POST, class Ckpt, bool COHERENT = false, bool STD = false,
+          bool TAPE = false>
 __device__ __forceinline__ void siso_window(const DevCb& cb, int w, int g, const SisoIo& io,
                                             const Ckpt& ck) {
-  siso_window_rt<S, Ckpt, COHERENT, STD>(cb, w, g, io, ck, LOWER, POST);
+  siso_window_rt<S, Ckpt, COHERENT, STD, false, TAPE>(cb, w, g, io, ck, LOWER, POST);
 }
 
 }  // namespace tcb
