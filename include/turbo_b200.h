@@ -320,8 +320,9 @@ TC_API int tc_decoder_timing(tc_decoder* dec, tc_timing* out, int reset);
  * 2*it+1 lower) multiplied by scales[j] before it becomes the other SISO's a-priori and before
  * it enters the posterior Ls + e1 + e2, run on the windowed schedule (window, guard;
  * 0 / -1 = 64 / 32; window >= K is the full trellis) whose next-iteration seeds are constants
- * of the function.  The adjoint is hand-written: alpha checkpointed at the window starts and
- * every 4 steps, recomputed on the backward pass, the transposed softmax weights of every max*.
+ * of the function.  The adjoint is hand-written: alpha checkpoints every 4 steps kept by the
+ * forward pass, beta checkpointed on the backward pass, both recomputed between checkpoints,
+ * the transposed softmax weights of every max*.
  * All buffers are device memory ordered on `stream` (NULL = the legacy default stream);
  * `scales` is host memory (2*iterations floats, NULL = all 1).  The LLR buffer must stay
  * unchanged between a forward pass and its backward pass.  A forward pass returns a tape id;
@@ -342,7 +343,8 @@ TC_API int tc_adjoint_forward_conv(int convention, tc_adjoint* adj, size_t n_cb,
                                    const float* scales, int32_t window, int32_t guard,
                                    void* stream, uint64_t* tape);
 /* grad_posterior: post_len floats (posterior layout); grad_llr: llr_len floats (LLR layout,
- * 0 outside every block); grad_scales: 2*iterations floats. */
+ * 0 outside every block; 16-byte aligned, as the LLR buffer); grad_scales: 2*iterations
+ * floats. */
 TC_API int tc_adjoint_backward(tc_adjoint* adj, uint64_t tape, const float* grad_posterior,
                                float* grad_llr, float* grad_scales, void* stream);
 TC_API int tc_adjoint_launches(tc_adjoint* adj, uint64_t* launches);

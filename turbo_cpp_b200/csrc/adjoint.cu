@@ -170,8 +170,8 @@ struct AdjIo {
   const float* llr;       // channel LLRs, [d0|d1|d2] per block
   const float* sys_i;     // interleaved systematic LLRs (work layout)
   const float* apr;       // the a-priori this SISO read in the forward pass (work layout)
-  const float* ge;        // d loss / d (scaled extrinsic of this SISO), work layout, natural order
-  const uint16_t* perm;   // lower SISO: position i's extrinsic is e2[perm[i]]
+  const float* ge;        // d loss / d (scaled extrinsic of this SISO), work layout, this SISO's
+                          // order (the lower SISO's: interleaved)
   const float* seeds;     // [launch window][16]: the seeds this SISO used
   float4* alpha_ckpt;     // the taped alpha checkpoints of this SISO: ckpt_slots planes of n_win
                           // float4 pairs, plane m = alpha at a_lo + 4m
@@ -194,18 +194,9 @@ __device__ __forceinline__ void load8(const float* p, float (&m)[8]) {
 }
 
 // d loss / d e of 4 consecutive positions of this SISO
-__device__ __forceinline__ void load_ge(const AdjIo& io, const DevCb& cb, bool lower, int q,
-                                        float (&ge)[4]) {
-  if (!lower) {
-    const float4 v = ld4(io.ge + cb.work + q);
-    ge[0] = v.x; ge[1] = v.y; ge[2] = v.z; ge[3] = v.w;
-  } else {
-    const uint2 iv = __ldg(reinterpret_cast<const uint2*>(io.perm + cb.tab + q));
-    ge[0] = __ldg(io.ge + cb.work + (iv.x & 0xffffu));
-    ge[1] = __ldg(io.ge + cb.work + (iv.x >> 16));
-    ge[2] = __ldg(io.ge + cb.work + (iv.y & 0xffffu));
-    ge[3] = __ldg(io.ge + cb.work + (iv.y >> 16));
-  }
+__device__ __forceinline__ void load_ge(const AdjIo& io, const DevCb& cb, int q, float (&ge)[4]) {
+  const float4 v = ld4(io.ge + cb.work + q);
+  ge[0] = v.x; ge[1] = v.y; ge[2] = v.z; ge[3] = v.w;
 }
 
 // PHASES: 1 = B, 2 = C, as separate launches (C reads what B stored in global memory): each
@@ -277,7 +268,7 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
     const int q = P - 4;
     scale4(load_raw4(sys, apr, par, q), sa, a, b);
     float ge[4];
-    load_ge(io, cb, LOWER, q, ge);
+    load_ge(io, cb, q, ge);
     float Al[4][8];
     cka.load((q - a_lo) >> 2, Al[0]);
 #pragma unroll
@@ -375,7 +366,7 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
     }
     const bool own = P < hi;
     float ge[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-    if (own) load_ge(io, cb, LOWER, P, ge);
+    if (own) load_ge(io, cb, P, ge);
     float gsa[4], gpar[4];
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
@@ -449,37 +440,50 @@ struct CombineIo {
   int64_t work;
   const float* guard_g;
   const float* tail_g;
-  const uint16_t* inv;     // lower SISO: natural position q is SISO position inv[q]
+  const uint16_t* perm;    // interleaved position i is natural position perm[i]
+  const uint16_t* inv;     // natural position q is interleaved position inv[q]
   const float* grad_post;  // posterior layout
   const float* win_part;   // [launch window]: this SISO's sum of ge * x per window
   float* grad_llr;         // LLR layout
-  float* ge_out;           // upper: d/d e2 of the previous iteration; lower: d/d e1 (natural)
+  float* ge_out;           // upper: d/d e2 of the previous iteration (interleaved order, as the
+                           // lower SISO reads it); lower: d/d e1 (natural order)
   double* cb_part;         // [code block]: the block's windows' win_part, summed in window order
 };
 
 constexpr int kMaxK = 6144;  // largest QPP block size
 constexpr int kCombineThreads = 256;
+constexpr int kCombineBatch = 2;
 
-// d loss / d(Ls+La) and d loss / d Lp at SISO position p: its own window's gradient, then the
-// alpha warm-up gradient of window w+1, then the beta warm-up gradient of window w-1 (a fixed
-// order, so the result is deterministic).
-__device__ __forceinline__ void position_grads(const CombineIo& c, const DevCb& cb, int p,
-                                               float& sa, float& par) {
+__device__ __forceinline__ float4 add4(float4 x, float4 y) {
+  return make_float4(x.x + y.x, x.y + y.y, x.z + y.z, x.w + y.w);
+}
+__device__ __forceinline__ float4 ldg4(const float* p) {
+  return __ldg(reinterpret_cast<const float4*>(p));
+}
+
+// d loss / d(Ls+La) and d loss / d Lp at SISO positions p..p+3 (p a multiple of 4, so all four
+// lie in one window and on the same side of every guard boundary, which are multiples of 8):
+// their own window's gradient (phase B's part plus phase C's), then the alpha warm-up gradient
+// of window w+1, then the beta warm-up gradient of window w-1 (a fixed order, so the result is
+// deterministic).
+__device__ __forceinline__ void position_grads4(const CombineIo& c, const DevCb& cb, int p,
+                                                float4& sa, float4& par) {
   const int W = cb.window, G = c.guard;
   const int w = p / W, lo = w * W;
-  sa = c.own_sa[cb.work + p] + c.own_sa[2 * c.work + cb.work + p];
-  par = c.own_par[cb.work + p] + c.own_par[2 * c.work + cb.work + p];
+  const int64_t o = cb.work + p;
+  sa = add4(ldg4(c.own_sa + o), ldg4(c.own_sa + 2 * c.work + o));
+  par = add4(ldg4(c.own_par + o), ldg4(c.own_par + 2 * c.work + o));
   if (w + 1 < cb.nwin && p >= lo + W - G) {
     const float* ag = c.guard_g + static_cast<int64_t>(4 * (cb.win0 + w + 1)) * G;
     const int j = p - (lo + W - G);
-    sa += ag[j];
-    par += ag[G + j];
+    sa = add4(sa, ldg4(ag + j));
+    par = add4(par, ldg4(ag + G + j));
   }
   if (w > 0 && p < lo + G) {
     const float* bg = c.guard_g + static_cast<int64_t>(4 * (cb.win0 + w - 1)) * G + 2 * G;
     const int j = p - lo;
-    sa += bg[j];
-    par += bg[G + j];
+    sa = add4(sa, ldg4(bg + j));
+    par = add4(par, ldg4(bg + G + j));
   }
 }
 
@@ -520,29 +524,44 @@ __device__ __forceinline__ void combine_tail(const CombineIo& c, const DevCb& cb
 }
 
 // One block per code block.  Adds the SISO's gradients to d0/d1 (upper, natural order) or to
-// d2 (lower, SISO order) and d0 (lower: staged in shared memory by SISO position, then gathered
-// through the inverse permutation so that every global access walks the natural order), writes
-// the adjoint of the a-priori (the other SISO's scaled extrinsic; plus d loss / d posterior for
-// the last lower SISO, whose extrinsic also enters the posterior), adds the tail gradients, and
-// sums the block's per-window scale parts in a fixed order.
+// d2 (lower, SISO order) and d0 (lower: gathered through the inverse permutation), and writes the
+// adjoint of the a-priori, the other SISO's scaled extrinsic, in that SISO's order (upper: the
+// lower SISO's interleaved order, gathered through the permutation; lower: natural order, plus
+// d loss / d posterior for the last lower SISO, whose extrinsic also enters the posterior).  The
+// gradients are staged in shared memory by this SISO's position, so that every global access
+// walks an order of its own.  Also adds the tail gradients and sums the block's per-window scale
+// parts in a fixed order.
 template <bool LOWER, bool LAST, bool STD = false>
 __global__ void __launch_bounds__(kCombineThreads) adj_combine_kernel(CombineIo c) {
-  __shared__ float sa_s[LOWER ? kMaxK : 1];
+  __shared__ __align__(16) float sa_s[kMaxK];
   __shared__ double red[kCombineThreads];
   for (int i = blockIdx.x; i < c.n_cb; i += gridDim.x) {
     const DevCb cb = c.cbs[i];
     const int K = cb.k;
     float* g0 = c.grad_llr + cb.llr;
-    for (int p = threadIdx.x; p < K; p += kCombineThreads) {
-      float sa, par;
-      position_grads(c, cb, p, sa, par);
-      if (!LOWER) {
-        g0[p] += sa;
-        g0[(K + 4) + p] += par;
-        c.ge_out[cb.work + p] = sa;
-      } else {
-        g0[2 * (K + 4) + p] += par;
-        sa_s[p] = sa;
+    // 4 consecutive positions per thread (float4; offsets are multiples of 4), kCombineBatch
+    // groups per pass, all loads before the stores
+    float4* s4 = reinterpret_cast<float4*>(sa_s);
+    float* gp = g0 + (LOWER ? 2 : 1) * (K + 4);  // parity: d1 (upper) or d2 (lower)
+    for (int p0 = 4 * threadIdx.x; p0 < K; p0 += 4 * kCombineThreads * kCombineBatch) {
+      float4 sa[kCombineBatch], par[kCombineBatch], g[kCombineBatch], h[kCombineBatch];
+#pragma unroll
+      for (int k = 0; k < kCombineBatch; ++k) {
+        const int p = p0 + 4 * k * kCombineThreads;
+        if (p < K) {
+          position_grads4(c, cb, p, sa[k], par[k]);
+          if (!LOWER) g[k] = *reinterpret_cast<const float4*>(g0 + p);
+          h[k] = *reinterpret_cast<const float4*>(gp + p);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kCombineBatch; ++k) {
+        const int p = p0 + 4 * k * kCombineThreads;
+        if (p < K) {
+          if (!LOWER) *reinterpret_cast<float4*>(g0 + p) = add4(g[k], sa[k]);
+          s4[p >> 2] = sa[k];
+          *reinterpret_cast<float4*>(gp + p) = add4(h[k], par[k]);
+        }
       }
     }
     if (threadIdx.x == 0) combine_tail<LOWER, STD>(c, cb, g0);
@@ -550,12 +569,40 @@ __global__ void __launch_bounds__(kCombineThreads) adj_combine_kernel(CombineIo 
     for (int v = threadIdx.x; v < cb.nwin; v += kCombineThreads) s += c.win_part[cb.win0 + v];
     red[threadIdx.x] = s;
     __syncthreads();
-    if (LOWER) {
+    if (!LOWER) {
+      const uint16_t* perm = c.perm + cb.tab;
+      for (int i = 4 * threadIdx.x; i < K; i += 4 * kCombineThreads) {
+        const uint2 v = __ldg(reinterpret_cast<const uint2*>(perm + i));
+        *reinterpret_cast<float4*>(c.ge_out + cb.work + i) =
+            make_float4(sa_s[v.x & 0xffffu], sa_s[v.x >> 16], sa_s[v.y & 0xffffu], sa_s[v.y >> 16]);
+      }
+    } else {
       const uint16_t* inv = c.inv + cb.tab;
-      for (int q = threadIdx.x; q < K; q += kCombineThreads) {
-        const float v = sa_s[inv[q]];
-        g0[q] += v;
-        c.ge_out[cb.work + q] = v + (LAST ? c.grad_post[cb.out + q] : 0.0f);
+      for (int q0 = 4 * threadIdx.x; q0 < K; q0 += 4 * kCombineThreads * kCombineBatch) {
+        float4 v[kCombineBatch], g[kCombineBatch];
+        float gq[kCombineBatch][4];
+#pragma unroll
+        for (int k = 0; k < kCombineBatch; ++k) {
+          const int q = q0 + 4 * k * kCombineThreads;
+          if (q < K) {
+            const uint2 iv = __ldg(reinterpret_cast<const uint2*>(inv + q));
+            v[k] = make_float4(sa_s[iv.x & 0xffffu], sa_s[iv.x >> 16], sa_s[iv.y & 0xffffu],
+                               sa_s[iv.y >> 16]);
+            g[k] = *reinterpret_cast<const float4*>(g0 + q);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) gq[k][e] = LAST ? c.grad_post[cb.out + q + e] : 0.0f;
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < kCombineBatch; ++k) {
+          const int q = q0 + 4 * k * kCombineThreads;
+          if (q < K) {
+            *reinterpret_cast<float4*>(g0 + q) = add4(g[k], v[k]);
+            *reinterpret_cast<float4*>(c.ge_out + cb.work + q) =
+                make_float4(v[k].x + gq[k][0], v[k].y + gq[k][1], v[k].z + gq[k][2],
+                            v[k].w + gq[k][3]);
+          }
+        }
       }
     }
     for (int o = kCombineThreads / 2; o > 0; o >>= 1) {
@@ -568,17 +615,16 @@ __global__ void __launch_bounds__(kCombineThreads) adj_combine_kernel(CombineIo 
 }
 
 // grad_llr: d0 gets d loss / d posterior (posterior = Ls + e1 + e2); ge2 = d loss / d e2 of the
-// last iteration (work layout).  grad_llr was zeroed before.
+// last iteration, in the lower SISO's (interleaved) order.  grad_llr was zeroed before.
 __global__ void adj_init_kernel(const DevCb* __restrict__ cbs, int n_cb,
-                                const float* __restrict__ grad_post, float* __restrict__ grad_llr,
-                                float* __restrict__ ge2) {
+                                const float* __restrict__ grad_post, const uint16_t* __restrict__ perm,
+                                float* __restrict__ grad_llr, float* __restrict__ ge2) {
   const int p = blockIdx.x * kSetupThreads + threadIdx.x;
   for (int i = blockIdx.y; i < n_cb; i += gridDim.y) {
     const DevCb cb = cbs[i];
     if (p < cb.k) {
-      const float gp = grad_post[cb.out + p];
-      grad_llr[cb.llr + p] = gp;
-      ge2[cb.work + p] = gp;
+      grad_llr[cb.llr + p] = grad_post[cb.out + p];
+      ge2[cb.work + p] = grad_post[cb.out + perm[cb.tab + p]];
     }
   }
 }
@@ -725,6 +771,8 @@ void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr
     throw InvalidArgument("the tape of this forward pass was replaced by a later forward pass");
   ok(cudaSetDevice(dec_.device()), "cudaSetDevice");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (reinterpret_cast<uintptr_t>(grad_llr) % 16 != 0)
+    throw InvalidArgument("grad_llr must be 16-byte aligned");
   const int64_t work = work_;
   const int n_win = n_win_, G = guard_;
   const uint32_t I = iterations_;
@@ -751,14 +799,14 @@ void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr
   const unsigned cb_blocks = static_cast<unsigned>(std::min(n, 1 << 20));
 
   ok(cudaMemsetAsync(grad_llr, 0, llr_len_ * sizeof(float), st), "zero grad_llr");
-  adj_init_kernel<<<pos_blocks, kSetupThreads, 0, st>>>(dcbs, n, grad_post, grad_llr, ge2);
+  adj_init_kernel<<<pos_blocks, kSetupThreads, 0, st>>>(dcbs, n, grad_post, dperm, grad_llr, ge2);
   ok(cudaGetLastError(), "adjoint init launch");
   launches_ += 1;
   const int blocks = (n_win + kAdjThreads - 1) / kAdjThreads;
   for (int j = static_cast<int>(2 * I) - 1; j >= 0; --j) {
     const bool lower = j & 1;
     const bool last = j + 2 >= static_cast<int>(2 * I);  // a SISO of the last iteration
-    AdjIo io{llr_, sysi, tape + j * work, lower ? ge2 : ga1, dperm, seeds + j * slab,
+    AdjIo io{llr_, sysi, tape + j * work, lower ? ge2 : ga1, seeds + j * slab,
              actp + j * aslab, own,
              own + work, work, guard_g, tail_g, part, ckpt, ckpt_bwd_,
              scales_[j], G};
@@ -778,7 +826,7 @@ void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr
       siso_adjoint_kernel<false, 2><<<blocks, kAdjThreads, 0, st>>>(dcbs, dwin, n_win, io);
     }
     ok(cudaGetLastError(), "SISO adjoint launch");
-    CombineIo c{dcbs, n, G, own, own + work, work, guard_g, tail_g, dinv, grad_post, part, grad_llr,
+    CombineIo c{dcbs, n, G, own, own + work, work, guard_g, tail_g, dperm, dinv, grad_post, part, grad_llr,
                 lower ? ga1 : ge2, cb_part + static_cast<int64_t>(j) * n};
     if (std3gpp_) {
       if (lower && last)
