@@ -151,6 +151,11 @@ def test_backward_is_deterministic_and_tapes_are_checked(tc, decoder):
     gs = torch.zeros(12, device="cuda")
     with pytest.raises(tc.InvalidArgument):
         adj.backward(t1, post.data_ptr(), g.data_ptr(), gs.data_ptr())
+    # grad_llr must be 16-byte aligned (the buffer is 4 floats longer, so a misaligned view
+    # would still lie inside it); the refusal comes before any launch
+    g_pad = torch.zeros(llr_len + 4, device="cuda")
+    with pytest.raises(tc.InvalidArgument):
+        adj.backward(t2, post.data_ptr(), g_pad.data_ptr() + 4, gs.data_ptr())
     adj.backward(t2, post.data_ptr(), g.data_ptr(), gs.data_ptr())
     torch.cuda.synchronize()
     with pytest.raises(tc.InvalidArgument):
