@@ -9,12 +9,12 @@
 //
 // Backward: per half-iteration, last to first, one thread per window of the forward schedule
 // runs the adjoint of its window in two phases (base-2 metrics, as the forward):
-//   B  backward in time from the beta start (seed or tail) to the alpha start: beta, stored
+//   1  backward in time from the beta start (seed or tail) to the alpha start: beta, stored
 //      every 4 steps; alpha recomputed from its checkpoint 4 steps at a time; the extrinsic's
 //      softmax weights give the direct alpha adjoint and d/d parity; the alpha adjoint
 //      recursion (transposed softmax weights of every max*) runs through the window and on
 //      through the alpha warm-up steps;
-//   C  forward in time from the window start to the beta start: beta recomputed from its
+//   2  forward in time from the window start to the beta start: beta recomputed from its
 //      checkpoints 4 steps at a time; the beta adjoint recursion, fed by the extrinsic's
 //      direct beta adjoint, runs through the window and the beta warm-up steps to the tail.
 // Per-step normalisations subtract a common value from all 8 metrics and every extrinsic is a
@@ -176,7 +176,7 @@ struct AdjIo {
   float4* alpha_ckpt;     // the taped alpha checkpoints of this SISO: ckpt_slots planes of n_win
                           // float4 pairs, plane m = alpha at a_lo + 4m
   float* own_sa;          // [work]: d loss / d(Ls+La) of the window's own steps (SISO order),
-                          // phase B's part; phase C's part follows at own_sa + 2 * work
+                          // phase 1's part; phase 2's part follows at own_sa + 2 * work
   float* own_par;         // [work]: d loss / d Lp (likewise)
   int64_t work;
   float* guard_g;         // [launch window][4][guard]: alpha warm-up sa, par; beta warm-up sa, par
@@ -199,7 +199,7 @@ __device__ __forceinline__ void load_ge(const AdjIo& io, const DevCb& cb, int q,
   ge[0] = v.x; ge[1] = v.y; ge[2] = v.z; ge[3] = v.w;
 }
 
-// PHASES: 1 = B, 2 = C, as separate launches (C reads what B stored in global memory): each
+// PHASES: 1 or 2, as separate launches (phase 2 reads what phase 1 stored in global memory): each
 // holds less live state, so that 6 blocks per SM (168 registers) fit where a single kernel held
 // 4 (234 registers).
 constexpr int kAdjMinBlocks = 6;
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
   const float xs = kLn2 * io.scale;  // d e / d(base-2 extrinsic)
 
   if (PHASES & 1) {
-  // ---- B: backward in time ----
+  // ---- phase 1: backward in time ----
   float be[8];
   if (tail) {
     float ts[3], tp[3];
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(kAdjThreads, kAdjMinBlocks) siso_adjoint_kerne
   }
 
   if (PHASES & 2) {
-  // ---- C: forward in time ----
+  // ---- phase 2: forward in time ----
   float bb[8], al[8], as[8];  // alpha in (m, s) form, advanced over the window's own steps
 #pragma unroll
   for (int s = 0; s < 8; ++s) bb[s] = 0.0f;
@@ -435,7 +435,7 @@ struct CombineIo {
   const DevCb* cbs;
   int n_cb;
   int guard;
-  const float* own_sa;     // phase B's own-step gradients; phase C's at + 2 * work
+  const float* own_sa;     // phase 1's own-step gradients; phase 2's at + 2 * work
   const float* own_par;
   int64_t work;
   const float* guard_g;
@@ -463,7 +463,7 @@ __device__ __forceinline__ float4 ldg4(const float* p) {
 
 // d loss / d(Ls+La) and d loss / d Lp at SISO positions p..p+3 (p a multiple of 4, so all four
 // lie in one window and on the same side of every guard boundary, which are multiples of 8):
-// their own window's gradient (phase B's part plus phase C's), then the alpha warm-up gradient
+// their own window's gradient (phase 1's part plus phase 2's), then the alpha warm-up gradient
 // of window w+1, then the beta warm-up gradient of window w-1 (a fixed order, so the result is
 // deterministic).
 __device__ __forceinline__ void position_grads4(const CombineIo& c, const DevCb& cb, int p,
