@@ -63,7 +63,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-configs", action="store_true",
-                    help="skip the config-3 (transport-block chain) and config-5 (mixed K) figures")
+                    help="skip the config-3 (transport-block chain), config-4 (differentiable "
+                         "decoder) and config-5 (mixed K) figures")
+    ap.add_argument("--configs", default="3,4,5",
+                    help="which of those figures to measure (comma-separated subset of 3,4,5)")
     return ap.parse_args()
 
 
@@ -821,9 +824,12 @@ def main():
     if e2e:
         line["e2e"] = e2e
     # ---- config 3 (transport-block chain) and config 5 (mixed K, early stop) figures ----
-    if not args.no_configs:
+    figs = set() if args.no_configs else {c.strip() for c in args.configs.split(",") if c.strip()}
+    if "3" in figs:
         line["config3_chain"] = config3_figure(tc, dev, stream, it)
+    if "5" in figs:
         line["config5_mixed"] = config5_figure(tc, dev, stream, it)
+    if "4" in figs:
         line["config4_adjoint"] = config4_figure(tc, dev)
 
     # ---- plain per-block GPU path: one code block per call, as the reference API decodes ----

@@ -27,84 +27,105 @@ struct DevRm {
   int64_t out;    // float offset of [d0|d1|d2] (3(K+4) floats)
 };
 
-constexpr int kRmThreads = kCircThreads;
+constexpr int kRmThreads = 1024;
+// largest circular buffer (K = 6144: 3 x 32 x 193 positions), floats
+constexpr int kMaxNcb = 3 * 32 * ((6144 + 4 + 31) / 32);
 
-// One CTA per code block.  The rate-matched LLR k lands on the k-th non-<NULL> position of the
-// circular walk that starts at k0; a valid position of rank r (valid positions before it) is
-// visited by k = (r - rank(k0)) mod Nv, then every Nv further LLRs.  Each stream element gathers
-// its visits in increasing k from 0.0f, which is the reference's summation order, so the result
-// is bit-identical to derate_match_streams with LLR values.
+// circular-buffer positions (floats of shared memory) of the largest block in `v`
+inline int max_ncb(const std::vector<DevRm>& v) {
+  int m = 0;
+  for (const DevRm& b : v) m = std::max(m, 3 * 32 * ((b.k + 4 + 31) / 32));
+  return m;
+}
+
+// acc[(r0 + kk) mod nv] += x[kk] for kk in [0, e), one round of nv LLRs at a time (each rank at
+// most once per round), so that every rank sums its LLRs in increasing kk -- the reference's
+// summation order.  Each thread requests kRmBatch LLRs before adding any (coalesced loads, kept in
+// flight together); consecutive kk hit consecutive shared-memory banks.  Ends with a barrier.
+constexpr int kRmBatch = 4;
+__device__ __forceinline__ void accumulate_rounds(float* acc, const float* __restrict__ x, int e,
+                                                  int nv, int r0) {
+  for (int base = 0; base < e; base += nv) {
+    const int n = min(nv, e - base);
+    for (int j0 = threadIdx.x; j0 < n; j0 += kRmThreads * kRmBatch) {
+      float v[kRmBatch];
+#pragma unroll
+      for (int u = 0; u < kRmBatch; ++u) {
+        const int j = j0 + u * kRmThreads;
+        v[u] = j < n ? __ldg(x + base + j) : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < kRmBatch; ++u) {
+        const int j = j0 + u * kRmThreads;
+        if (j < n) {
+          int r = r0 + j;
+          if (r >= nv) r -= nv;
+          acc[r] += v[u];
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// One CTA per code block.  The rate-matched LLR kk lands on the valid circular-buffer position of
+// rank (rank(k0) + kk) mod Nv: the LLRs are summed per rank in shared memory (coalesced reads,
+// increasing kk from 0.0f, the reference's order, so the result is bit-identical to
+// derate_match_streams with LLR values), then every [d0|d1|d2] element takes the sum of its
+// position's rank (closed form, CircularRank; coalesced stores); the filler elements of d0 and
+// d1 (<NULL> in the buffer) are 0.  Dynamic shared memory: Ncb floats of the largest block.
 __global__ void __launch_bounds__(kRmThreads) derate_llr_kernel(const DevRm* __restrict__ blocks,
                                                                 const float* __restrict__ e_llr,
                                                                 float* __restrict__ d012) {
-  __shared__ int warp_sum[kRmThreads / 32];
-  __shared__ int s_rank_k0, s_total;
+  extern __shared__ float acc[];
+  __shared__ int tables[kRankTableInts];
   const DevRm b = blocks[blockIdx.x];
-  CircularScan cs(b.k, b.filler);
-  float* out = d012 + b.out;
-  // every position of [d0|d1|d2] is a valid buffer position, written below, except the filler
-  // positions of d0 and d1 (<NULL> in the buffer), which de-rate matching sets to 0
-  for (int i = threadIdx.x; i < cs.filler; i += blockDim.x) out[i] = out[cs.d + i] = 0.0f;
-  cs.scan(warp_sum, &s_total);
-  cs.rank_of(cs.k0(b.rv), &s_rank_k0);
+  CircularRank cr(b.k, b.filler, tables);
+  cr.setup();
+  for (int j = threadIdx.x; j < cr.ncb; j += kRmThreads) acc[j] = 0.0f;
   __syncthreads();
-  const int nv = s_total, r0 = s_rank_k0;
-  const float* x = e_llr + b.e_off;
-  int rank = cs.before;
-  CircularWalk wk = cs.walk(cs.p0);
-  for (int p = cs.p0; p < cs.p1; ++p) {
-    const int src = wk.next();
-    if (src < 0) continue;
-    int kk = rank - r0;
-    if (kk < 0) kk += nv;
-    float sum = 0.0f;
-    for (; kk < b.e; kk += nv) sum += x[kk];
-    out[src] = sum;
-    ++rank;
+  accumulate_rounds(acc, e_llr + b.e_off, b.e, cr.valid(), cr.rank(cr.k0(b.rv)));
+  float* out = d012 + b.out;
+  for (int i = threadIdx.x; i < 3 * cr.d; i += kRmThreads) {
+    const int r = cr.rank_of_element(i);
+    out[i] = r >= 0 ? acc[r] : 0.0f;
   }
 }
 
 // HARQ soft combining: one CTA per code block, whose transmissions (up to kMaxHarqTx, each with
 // its own rv, E and rate-matched LLRs) are consecutive in `tx`.  The ranks of the valid
-// circular-buffer positions depend only on K and the filler count, so one scan serves every
-// transmission; each stream element sums each transmission's visits in increasing k from 0.0f
-// (that transmission's de-rate-matched value, as derate_llr_kernel) and adds the transmissions
-// in their order -- bit-identical to de-rate matching each transmission alone and adding the
-// results in that order.
+// circular-buffer positions depend only on K and the filler count; each transmission's LLRs are
+// summed per rank in increasing kk from 0.0f (its de-rate-matched value, as derate_llr_kernel)
+// and added to the total in transmission order -- bit-identical to de-rate matching each
+// transmission alone and adding the results in that order.  Dynamic shared memory: 2 Ncb floats
+// of the largest block.
 constexpr int kMaxHarqTx = 8;
 
 __global__ void __launch_bounds__(kRmThreads) derate_combine_kernel(
     const DevRm* __restrict__ tx, const int32_t* __restrict__ group_first,
     const float* __restrict__ e_llr, float* __restrict__ d012) {
-  __shared__ int warp_sum[kRmThreads / 32];
-  __shared__ int s_rank_k0[kMaxHarqTx], s_total;
+  extern __shared__ float acc[];  // [0, Ncb): the total; [Ncb, 2 Ncb): one transmission
+  __shared__ int tables[kRankTableInts];
   const int t0 = group_first[blockIdx.x], nt = group_first[blockIdx.x + 1] - t0;
   const DevRm b = tx[t0];
-  CircularScan cs(b.k, b.filler);
-  float* out = d012 + b.out;
-  // every position of [d0|d1|d2] is a valid buffer position, written below, except the filler
-  // positions of d0 and d1 (<NULL> in the buffer), which de-rate matching sets to 0
-  for (int i = threadIdx.x; i < cs.filler; i += blockDim.x) out[i] = out[cs.d + i] = 0.0f;
-  cs.scan(warp_sum, &s_total);
-  for (int t = 0; t < nt; ++t) cs.rank_of(cs.k0(tx[t0 + t].rv), &s_rank_k0[t]);
+  CircularRank cr(b.k, b.filler, tables);
+  cr.setup();
+  float* part = acc + cr.ncb;
+  for (int j = threadIdx.x; j < cr.ncb; j += kRmThreads) acc[j] = 0.0f;
   __syncthreads();
-  const int nv = s_total;
-  int rank = cs.before;
-  CircularWalk wk = cs.walk(cs.p0);
-  for (int p = cs.p0; p < cs.p1; ++p) {
-    const int src = wk.next();
-    if (src < 0) continue;
-    float acc = 0.0f;
-    for (int t = 0; t < nt; ++t) {
-      const DevRm& x = tx[t0 + t];
-      int kk = rank - s_rank_k0[t];
-      if (kk < 0) kk += nv;
-      float part = 0.0f;
-      for (; kk < x.e; kk += nv) part += e_llr[x.e_off + kk];
-      acc += part;
-    }
-    out[src] = acc;
-    ++rank;
+  const int nv = cr.valid();
+  for (int t = 0; t < nt; ++t) {
+    const DevRm x = tx[t0 + t];
+    for (int j = threadIdx.x; j < nv; j += kRmThreads) part[j] = 0.0f;
+    __syncthreads();
+    accumulate_rounds(part, e_llr + x.e_off, x.e, nv, cr.rank(cr.k0(x.rv)));
+    for (int j = threadIdx.x; j < nv; j += kRmThreads) acc[j] += part[j];
+    __syncthreads();
+  }
+  float* out = d012 + b.out;
+  for (int i = threadIdx.x; i < 3 * cr.d; i += kRmThreads) {
+    const int r = cr.rank_of_element(i);
+    out[i] = r >= 0 ? acc[r] : 0.0f;
   }
 }
 
@@ -212,6 +233,17 @@ std::vector<uint32_t> xpow_table(CrcKind kind, size_t n, Convention conv) {
 
 }  // namespace
 
+// The de-rate kernels' shared memory above the default 48 KB: Ncb floats of the largest block
+// (two buffers for HARQ combining).
+void configure_chain_kernels() {
+  check(cudaFuncSetAttribute(derate_llr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kMaxNcb * static_cast<int>(sizeof(float))),
+        "de-rate smem attr");
+  check(cudaFuncSetAttribute(derate_combine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             2 * kMaxNcb * static_cast<int>(sizeof(float))),
+        "combine smem attr");
+}
+
 // d012 = de-rate-matched LLRs of every block ([d0|d1|d2] each, at blocks[i].llr_offset).
 void Decoder::derate_device(size_t n, const RmBlockDesc* blocks, const float* e_llr, size_t e_len,
                             float* d012, size_t llr_len, void* stream) {
@@ -231,8 +263,8 @@ void Decoder::derate_device(size_t n, const RmBlockDesc* blocks, const float* e_
   if (n == 0) return;
   DevRm* d = grow<DevRm>(d_rm_, n);
   upload(d, v.data(), n * sizeof(DevRm), stream);
-  derate_llr_kernel<<<static_cast<unsigned>(n), kRmThreads, 0, static_cast<cudaStream_t>(stream)>>>(
-      d, e_llr, d012);
+  derate_llr_kernel<<<static_cast<unsigned>(n), kRmThreads, max_ncb(v) * sizeof(float),
+                      static_cast<cudaStream_t>(stream)>>>(d, e_llr, d012);
   check(cudaGetLastError(), "de-rate launch");
   timing_.launches += 1;
 }
@@ -272,8 +304,9 @@ void Decoder::derate_combine_llr(size_t n, const RmBlockDesc* tx, const float* e
   int32_t* g = grow<int32_t>(d_rmgroup_, groups + 1);
   upload(d, v.data(), n * sizeof(DevRm), stream);
   upload(g, first.data(), (groups + 1) * sizeof(int32_t), stream);
-  derate_combine_kernel<<<static_cast<unsigned>(groups), kRmThreads, 0,
-                          static_cast<cudaStream_t>(stream)>>>(d, g, e_llr, d012);
+  derate_combine_kernel<<<static_cast<unsigned>(groups), kRmThreads,
+                          2 * max_ncb(v) * sizeof(float), static_cast<cudaStream_t>(stream)>>>(
+      d, g, e_llr, d012);
   check(cudaGetLastError(), "combine launch");
   timing_.launches += 1;
   mark_done(stream);

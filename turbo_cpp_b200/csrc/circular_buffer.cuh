@@ -13,8 +13,11 @@
 namespace tcb {
 namespace {
 
-__constant__ uint8_t c_col_perm[32] = {0, 16, 8, 24, 4, 20, 12, 28, 2, 18, 10, 26, 6, 22, 14, 30,
-                                       1, 17, 9, 25, 5, 21, 13, 29, 3, 19, 11, 27, 7, 23, 15, 31};
+// The inter-column permutation of the sub-block interleaver (TS 36.212 Table 5.1.4-1,
+// lte_turbo.cpp:195-236) is the 5-bit reversal of the column index, its own inverse: one
+// instruction, where a table in constant memory would serialise a warp whose lanes read
+// different columns.
+__device__ __forceinline__ int col_perm(int c) { return static_cast<int>(__brev(static_cast<unsigned>(c)) >> 27); }
 
 constexpr int kCircThreads = 512;  // threads per CTA of the kernels that use CircularScan
 
@@ -23,15 +26,15 @@ constexpr int kCircThreads = 512;  // threads per CTA of the kernels that use Ci
 __device__ __forceinline__ int rm_source(int pos, int d, int rows, int kpi, int filler) {
   const int dummy = kpi - d;
   if (pos < kpi) {  // systematic, read column by column
-    const int y = (pos % rows) * 32 + c_col_perm[pos / rows] - dummy;
+    const int y = (pos % rows) * 32 + col_perm(pos / rows) - dummy;
     return (y < 0 || y < filler) ? -1 : y;
   }
   const int local = pos - kpi, lane = local >> 1;
   if ((local & 1) == 0) {  // parity 1: same permutation as the systematic stream
-    const int y = (lane % rows) * 32 + c_col_perm[lane / rows] - dummy;
+    const int y = (lane % rows) * 32 + col_perm(lane / rows) - dummy;
     return (y < 0 || y < filler) ? -1 : d + y;
   }
-  const int y = (c_col_perm[lane / rows] + 32 * (lane % rows) + 1) % kpi - dummy;
+  const int y = (col_perm(lane / rows) + 32 * (lane % rows) + 1) % kpi - dummy;
   return y < 0 ? -1 : 2 * d + y;  // parity 2: no filler nulling
 }
 
@@ -53,7 +56,7 @@ struct CircularWalk {
   __device__ __forceinline__ int next() {
     int src;
     if (pos < kpi) {  // systematic, read column by column
-      const int y = r * 32 + c_col_perm[q] - dummy;
+      const int y = r * 32 + col_perm(q) - dummy;
       src = (y < 0 || y < filler) ? -1 : y;
       if (++r == rows) {
         r = 0;
@@ -63,10 +66,10 @@ struct CircularWalk {
       return src;
     }
     if (((pos - kpi) & 1) == 0) {  // parity 1: same permutation as the systematic stream
-      const int y = r * 32 + c_col_perm[q] - dummy;
+      const int y = r * 32 + col_perm(q) - dummy;
       src = (y < 0 || y < filler) ? -1 : d + y;
     } else {  // parity 2: no filler nulling; the lane advances after its second stream
-      int y = c_col_perm[q] + 32 * r + 1;
+      int y = col_perm(q) + 32 * r + 1;
       if (y >= kpi) y -= kpi;
       y -= dummy;
       src = y < 0 ? -1 : 2 * d + y;
@@ -148,6 +151,92 @@ struct CircularScan {
       for (int p = p0; p < pos; ++p) r += wk.next() >= 0;
       *out = r;
     }
+  }
+};
+
+// The ranks of circular-buffer positions in closed form, and each [d0|d1|d2] element's
+// position.  The column permutation of the sub-block interleaver is a 5-bit reversal, its own
+// inverse.  In a column q (32 columns of `rows` rows, read top to bottom) the <NULL> entries of
+// the systematic stream and of parity 1 are the top rows r with r*32 + perm[q] < dummy + filler
+// (cnt1[q] of them); parity 2 is <NULL> in row 0 when perm[q] + 1 < dummy and in the last row of
+// the column with perm[q] = 31 when dummy > 0 (its index wraps to 0).  The <NULL> entries before
+// a position are therefore a prefix over whole columns plus a count inside its column, and
+// rank(p) = p - that number.  setup() is run by the first warp of the CTA (tables in shared
+// memory: kRankTableInts ints), followed by a barrier.
+constexpr int kRankTableInts = 32 + 2 * 33;
+struct CircularRank {
+  int d, rows, kpi, ncb, filler, dummy;
+  int* cnt1;   // [32]: <NULL> rows at the top of column q (systematic, parity 1)
+  int* pre1;   // [33]: prefix of cnt1 over the columns
+  int* pre12;  // [33]: prefix of cnt1 + the parity-2 <NULL>s over the columns
+
+  __device__ __forceinline__ CircularRank(int k, int filler_bits, int* smem)
+      : d(k + 4), rows((k + 4 + 31) / 32), filler(filler_bits), cnt1(smem), pre1(smem + 32),
+        pre12(smem + 65) {
+    kpi = rows * 32;
+    ncb = 3 * kpi;
+    dummy = kpi - d;
+  }
+
+  __device__ __forceinline__ bool p2_row0_null(int q) const { return col_perm(q) + 1 < dummy; }
+
+  // first warp: the per-column tables
+  __device__ __forceinline__ void setup() {
+    if (threadIdx.x >= 32) return;
+    const int q = threadIdx.x, pq = col_perm(q);
+    const int t = dummy + filler - pq;
+    const int c1 = t <= 0 ? 0 : min(rows, (t + 31) >> 5);
+    const int c2 = (pq + 1 < dummy ? 1 : 0) + (pq == 31 && dummy > 0 ? 1 : 0);
+    cnt1[q] = c1;
+    int a = c1, b = c1 + c2;  // inclusive prefixes over columns 0..q
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int ua = __shfl_up_sync(0xffffffffu, a, o), ub = __shfl_up_sync(0xffffffffu, b, o);
+      if (q >= o) {
+        a += ua;
+        b += ub;
+      }
+    }
+    pre1[q + 1] = a;
+    pre12[q + 1] = b;
+    if (q == 0) pre1[0] = pre12[0] = 0;
+  }
+
+  __device__ __forceinline__ int valid() const { return ncb - pre1[32] - pre12[32]; }  // Nv
+  // rank of the systematic position of column q, row r
+  __device__ __forceinline__ int rank_sys(int q, int r) const {
+    return q * rows + r - (pre1[q] + min(r, cnt1[q]));
+  }
+  // rank of the parity-1 (odd = 0) or parity-2 (odd = 1) position of lane (q, r)
+  __device__ __forceinline__ int rank_par(int q, int r, int odd) const {
+    const int nulls = pre1[32] + pre12[q] + min(r, cnt1[q]) + (r > 0 && p2_row0_null(q) ? 1 : 0) +
+                      (odd && r < cnt1[q] ? 1 : 0);
+    return kpi + 2 * (q * rows + r) + odd - nulls;
+  }
+  // rank of any position p in [0, Ncb) (valid positions before it)
+  __device__ __forceinline__ int rank(int p) const {
+    if (p < kpi) return rank_sys(p / rows, p % rows);
+    const int lane = (p - kpi) >> 1;
+    return rank_par(lane / rows, lane % rows, (p - kpi) & 1);
+  }
+  // the rank of [d0|d1|d2] element i (stream i / d), or -1 for the filler elements of d0 and d1
+  // (<NULL> in the buffer)
+  __device__ __forceinline__ int rank_of_element(int i) const {
+    const int s = i >= d ? (i >= 2 * d ? 2 : 1) : 0;
+    const int y = i - s * d;
+    if (s < 2) {
+      if (y < filler) return -1;
+      const int yy = y + dummy;
+      const int q = col_perm(yy & 31), r = yy >> 5;
+      return s == 0 ? rank_sys(q, r) : rank_par(q, r, 0);
+    }
+    const int y2 = y + dummy;
+    const int v = y2 > 0 ? y2 - 1 : kpi - 1;
+    return rank_par(col_perm(v & 31), v >> 5, 1);
+  }
+  // k0 of redundancy version rv (lte_turbo.cpp:294-295), reduced modulo Ncb
+  __device__ __forceinline__ int k0(int rv) const {
+    return rows * (2 * ((ncb + 8 * rows - 1) / (8 * rows)) * rv + 2) % ncb;
   }
 };
 

@@ -156,6 +156,7 @@ Decoder::Decoder(int device) : device_(device) {
                         reinterpret_cast<const void*>(persistent_kernel<true>)})
     check(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 0),
           "carveout attr");
+  configure_chain_kernels();
   int per_sm_std = 0;
   check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_std, persistent_kernel<true>,
                                                       kPersistThreads, 0),

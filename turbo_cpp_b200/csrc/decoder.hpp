@@ -266,6 +266,9 @@ class Decoder {
 
 // The kernels index a checkpoint slab (windows interleaved, siso.cuh CkptStrided) with 32-bit
 // plane offsets: a call whose slab would reach 2^31 float4 (32 GB) is refused.
+// Kernel attributes of the transport-block chain (chain.cu); the decoder sets them on its device.
+void configure_chain_kernels();
+
 inline size_t ckpt_slab(size_t n_win, size_t planes) {
   const size_t n = n_win * planes;
   if (n >= (size_t{1} << 31))
