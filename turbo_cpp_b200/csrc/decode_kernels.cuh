@@ -48,29 +48,43 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) siso_plain_kernel(const 
   }
 }
 
-// sys_i[i] = d0[Pi(i)]; E2 = 0 (first a-priori).  The grid's y index walks the code blocks and
-// its x index the positions of one block (24 x 256 threads cover the largest K), so no thread
-// has to search for its block.
+// The grid of the per-position kernels (adjoint initialisation): the y index walks the code
+// blocks and the x index (24 x 256 threads cover the largest K) the positions of one block.
 constexpr int kSetupThreads = 256;
 constexpr int kSetupBlocksPerCb = (6144 + kSetupThreads - 1) / kSetupThreads;
-__global__ void setup_kernel(const DevCb* __restrict__ cbs, int n_cb, const float* __restrict__ llr,
-                             const uint16_t* __restrict__ perm, float* __restrict__ sys_i,
-                             float* __restrict__ e2) {
-  const int p = blockIdx.x * kSetupThreads + threadIdx.x;
-  for (int c = blockIdx.y; c < n_cb; c += gridDim.y) {
+
+// sys_i[i] = d0[Pi(i)]; E2 = 0 (first a-priori).  One CTA per code block: d0 is read into shared
+// memory with coalesced loads, then the interleaved copy is gathered from there, so that every
+// global access walks its array in order (a direct gather would read one 32-byte sector per
+// 4-byte element).
+constexpr int kGatherThreads = 512;
+constexpr int kMaxBlockK = 6144;
+__global__ void __launch_bounds__(kGatherThreads) setup_kernel(const DevCb* __restrict__ cbs,
+                                                               int n_cb,
+                                                               const float* __restrict__ llr,
+                                                               const uint16_t* __restrict__ perm,
+                                                               float* __restrict__ sys_i,
+                                                               float* __restrict__ e2) {
+  __shared__ float d0[kMaxBlockK];
+  for (int c = blockIdx.x; c < n_cb; c += gridDim.x) {
     const DevCb cb = cbs[c];
-    if (p < cb.k) {
-      sys_i[cb.work + p] = llr[cb.llr + perm[cb.tab + p]];
+    const float* src = llr + cb.llr;
+    for (int p = threadIdx.x; p < cb.k; p += kGatherThreads) d0[p] = __ldg(src + p);
+    __syncthreads();
+    const uint16_t* pi = perm + cb.tab;
+    for (int p = threadIdx.x; p < cb.k; p += kGatherThreads) {
+      sys_i[cb.work + p] = d0[pi[p]];
       e2[cb.work + p] = 0.0f;
     }
+    __syncthreads();  // d0 is reused by the next code block
   }
 }
 
 inline void launch_setup(const DevCb* cbs, int n_cb, const float* llr, const uint16_t* perm,
                          float* sys_i, float* e2, cudaStream_t st) {
   if (n_cb <= 0) return;
-  const dim3 grid(kSetupBlocksPerCb, static_cast<unsigned>(n_cb < 65535 ? n_cb : 65535));
-  setup_kernel<<<grid, kSetupThreads, 0, st>>>(cbs, n_cb, llr, perm, sys_i, e2);
+  const unsigned grid = static_cast<unsigned>(n_cb < (1 << 20) ? n_cb : (1 << 20));
+  setup_kernel<<<grid, kGatherThreads, 0, st>>>(cbs, n_cb, llr, perm, sys_i, e2);
 }
 
 // CRC24B early stop (lte_turbo.cpp:792-804): hard decisions (>= 0 -> 1) of bits
