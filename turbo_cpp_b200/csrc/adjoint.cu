@@ -452,7 +452,7 @@ struct CombineIo {
 
 constexpr int kMaxK = 6144;  // largest QPP block size
 constexpr int kCombineThreads = 256;
-constexpr int kCombineBatch = 2;
+constexpr int kCombineBatch = 1;  // measured best of 1, 2, 4 (registers against loads in flight)
 
 __device__ __forceinline__ float4 add4(float4 x, float4 y) {
   return make_float4(x.x + y.x, x.y + y.y, x.z + y.z, x.w + y.w);
@@ -615,17 +615,24 @@ __global__ void __launch_bounds__(kCombineThreads) adj_combine_kernel(CombineIo 
 }
 
 // grad_llr: d0 gets d loss / d posterior (posterior = Ls + e1 + e2); ge2 = d loss / d e2 of the
-// last iteration, in the lower SISO's (interleaved) order.  grad_llr was zeroed before.
-__global__ void adj_init_kernel(const DevCb* __restrict__ cbs, int n_cb,
-                                const float* __restrict__ grad_post, const uint16_t* __restrict__ perm,
-                                float* __restrict__ grad_llr, float* __restrict__ ge2) {
-  const int p = blockIdx.x * kSetupThreads + threadIdx.x;
-  for (int i = blockIdx.y; i < n_cb; i += gridDim.y) {
+// last iteration, in the lower SISO's (interleaved) order.  grad_llr was zeroed before.  One CTA
+// per code block: the block's d loss / d posterior is staged in shared memory and gathered
+// through the permutation from there, so that every global access walks its array in order.
+__global__ void __launch_bounds__(kCombineThreads) adj_init_kernel(
+    const DevCb* __restrict__ cbs, int n_cb, const float* __restrict__ grad_post,
+    const uint16_t* __restrict__ perm, float* __restrict__ grad_llr, float* __restrict__ ge2) {
+  __shared__ float gp[kMaxK];
+  for (int i = blockIdx.x; i < n_cb; i += gridDim.x) {
     const DevCb cb = cbs[i];
-    if (p < cb.k) {
-      grad_llr[cb.llr + p] = grad_post[cb.out + p];
-      ge2[cb.work + p] = grad_post[cb.out + perm[cb.tab + p]];
+    for (int p = threadIdx.x; p < cb.k; p += kCombineThreads) {
+      const float v = grad_post[cb.out + p];
+      gp[p] = v;
+      grad_llr[cb.llr + p] = v;
     }
+    __syncthreads();
+    const uint16_t* pi = perm + cb.tab;
+    for (int p = threadIdx.x; p < cb.k; p += kCombineThreads) ge2[cb.work + p] = gp[pi[p]];
+    __syncthreads();  // gp is reused by the next code block
   }
 }
 
@@ -795,11 +802,10 @@ void Adjoint::backward(uint64_t tape_id, const float* grad_post, float* grad_llr
   const uint16_t* dperm = dec_.perm_table();
   const uint16_t* dinv = dec_.inv_table();
   const int n = static_cast<int>(n_cb_);
-  const dim3 pos_blocks(kSetupBlocksPerCb, static_cast<unsigned>(n < 65535 ? n : 65535));
   const unsigned cb_blocks = static_cast<unsigned>(std::min(n, 1 << 20));
 
   ok(cudaMemsetAsync(grad_llr, 0, llr_len_ * sizeof(float), st), "zero grad_llr");
-  adj_init_kernel<<<pos_blocks, kSetupThreads, 0, st>>>(dcbs, n, grad_post, dperm, grad_llr, ge2);
+  adj_init_kernel<<<cb_blocks, kCombineThreads, 0, st>>>(dcbs, n, grad_post, dperm, grad_llr, ge2);
   ok(cudaGetLastError(), "adjoint init launch");
   launches_ += 1;
   const int blocks = (n_win + kAdjThreads - 1) / kAdjThreads;

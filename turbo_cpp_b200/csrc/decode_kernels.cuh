@@ -48,11 +48,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) siso_plain_kernel(const 
   }
 }
 
-// The grid of the per-position kernels (adjoint initialisation): the y index walks the code
-// blocks and the x index (24 x 256 threads cover the largest K) the positions of one block.
-constexpr int kSetupThreads = 256;
-constexpr int kSetupBlocksPerCb = (6144 + kSetupThreads - 1) / kSetupThreads;
-
 // sys_i[i] = d0[Pi(i)]; E2 = 0 (first a-priori).  One CTA per code block: d0 is read into shared
 // memory with coalesced loads, then the interleaved copy is gathered from there, so that every
 // global access walks its array in order (a direct gather would read one 32-byte sector per
