@@ -35,27 +35,10 @@ void check(cudaError_t e, const char* what) {
 
 }  // namespace
 
-// Pops the staging regions whose copies have completed (all of them, waiting, if wait_all).
-void Decoder::stage_retire(bool wait_all) {
-  while (!stage_busy_.empty()) {
-    cudaEvent_t e = static_cast<cudaEvent_t>(stage_busy_.front().event);
-    if (wait_all) {
-      check(cudaEventSynchronize(e), "cudaEventSynchronize");
-    } else {
-      const cudaError_t q = cudaEventQuery(e);
-      if (q == cudaErrorNotReady) break;
-      check(q, "cudaEventQuery");
-    }
-    stage_events_.push_back(e);
-    stage_busy_.pop_front();
-  }
-}
-
 void Decoder::upload(void* dst, const void* src, size_t bytes, void* stream) {
   if (bytes == 0) return;
   const size_t padded = (bytes + 255) & ~size_t{255};
   upload_bytes_ += padded;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (capturing_ != nullptr) {  // the graph reads its own pinned copy at every replay
     GraphEntry& g = *capturing_;
     if (g.arena_used + padded > g.arena_bytes)
@@ -63,40 +46,10 @@ void Decoder::upload(void* dst, const void* src, size_t bytes, void* stream) {
     char* pinned = static_cast<char*>(g.arena) + g.arena_used;
     g.arena_used += padded;
     std::memcpy(pinned, src, bytes);
-    check(cudaMemcpyAsync(dst, pinned, bytes, cudaMemcpyHostToDevice, st), "copy descriptors");
-    return;
+    src = pinned;
   }
-  stage_retire(false);
-  if (2 * padded > stage_bytes_) {  // grow: every earlier copy out of the old ring completes first
-    stage_retire(true);
-    if (stage_) check(cudaFreeHost(stage_), "cudaFreeHost");
-    stage_ = nullptr;
-    stage_bytes_ = stage_head_ = 0;
-    const size_t want = std::max<size_t>(4 * padded, size_t{8} << 20);
-    check(cudaMallocHost(&stage_, want), "cudaMallocHost");
-    stage_bytes_ = want;
-  }
-  if (stage_head_ + padded > stage_bytes_) stage_head_ = 0;
-  const size_t lo = stage_head_, hi = lo + padded;
-  while (!stage_busy_.empty() && stage_busy_.front().lo < hi && lo < stage_busy_.front().hi) {
-    cudaEvent_t e = static_cast<cudaEvent_t>(stage_busy_.front().event);
-    check(cudaEventSynchronize(e), "cudaEventSynchronize");
-    stage_events_.push_back(e);
-    stage_busy_.pop_front();
-  }
-  char* pinned = static_cast<char*>(stage_) + lo;
-  std::memcpy(pinned, src, bytes);
-  check(cudaMemcpyAsync(dst, pinned, bytes, cudaMemcpyHostToDevice, st), "copy descriptors");
-  cudaEvent_t e;
-  if (stage_events_.empty()) {
-    check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
-  } else {
-    e = static_cast<cudaEvent_t>(stage_events_.back());
-    stage_events_.pop_back();
-  }
-  check(cudaEventRecord(e, st), "cudaEventRecord");
-  stage_busy_.push_back(StageUse{lo, hi, e});
-  stage_head_ = hi;
+  check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, static_cast<cudaStream_t>(stream)),
+        "copy descriptors");
 }
 
 void Decoder::drop_graph(GraphEntry& e) {
@@ -216,12 +169,6 @@ Decoder::Decoder(int device) : device_(device) {
 
 Decoder::~Decoder() {
   cudaSetDevice(device_);
-  for (auto& u : stage_busy_) {  // copies out of the staging ring complete before it is freed
-    cudaEventSynchronize(static_cast<cudaEvent_t>(u.event));
-    cudaEventDestroy(static_cast<cudaEvent_t>(u.event));
-  }
-  for (void* e : stage_events_) cudaEventDestroy(static_cast<cudaEvent_t>(e));
-  if (stage_) cudaFreeHost(stage_);
   for (auto& g : graphs_) drop_graph(g);
   if (last_event_) cudaEventDestroy(static_cast<cudaEvent_t>(last_event_));
   if (compute_done_) cudaEventDestroy(static_cast<cudaEvent_t>(compute_done_));

@@ -192,22 +192,8 @@ class Decoder {
   std::vector<std::unique_ptr<Decoder>> workers_;
   size_t next_worker_ = 0;
   void decode_graph(const DecodeRequest& rq);
-  // host -> device copy of launch descriptors, staged in pinned memory so that the copy is
-  // asynchronous (a copy from pageable memory would first wait for all earlier work of the
-  // stream): while capturing, the graph's own arena; otherwise the staging ring below
+  // host -> device copy of launch descriptors; while capturing, from graph-owned pinned memory
   void upload(void* dst, const void* src, size_t bytes, void* stream);
-  // Staging ring of the uncaptured uploads: a region is written again only after the event
-  // recorded behind its copy has completed (busy regions, oldest first, lie in ring order after
-  // the head, so the oldest is the first that a new region can reach).
-  struct StageUse {
-    size_t lo, hi;
-    void* event;  // cudaEvent_t
-  };
-  void* stage_ = nullptr;
-  size_t stage_bytes_ = 0, stage_head_ = 0;
-  std::list<StageUse> stage_busy_;
-  std::vector<void*> stage_events_;  // free events
-  void stage_retire(bool wait_all);
   template <class T>
   T* grow(DeviceBuffer& b, size_t count) {
     void* before = b.ptr;
