@@ -128,7 +128,10 @@ typedef struct {
 } tc_code_block;
 
 /* HOST: synchronous, the call copies the LLRs in and the results out.  DEVICE: device pointers,
- * ordered on opts->stream, returns once enqueued.  HOST_ASYNC (new): host pointers; the call
+ * ordered on opts->stream, returns once enqueued (without a graph replay, the launch
+ * descriptors' copy first waits for the work already on that stream, so back-to-back calls
+ * return as each previous one finishes; a replayed graph never waits).  HOST_ASYNC (new): host
+ * pointers; the call
  * enqueues copy-in, decode and copy-out on one of three internal device workspaces (used in
  * turn, each with its own stream) and returns, so that one call's copies run while earlier
  * calls decode; results are valid, and the input buffer may be reused, after tc_decoder_sync.
@@ -196,7 +199,8 @@ TC_API int tc_decoder_inject_stall(tc_decoder* dec, int task);
 
 /* Decodes n_cb code blocks.  llr has llr_len floats, posterior post_len floats; crc_ok
  * (n_cb bytes) and iterations_used (n_cb words) may be NULL.  With TC_MEM_HOST the call is
- * synchronous; with TC_MEM_DEVICE it is ordered on opts->stream and returns once enqueued. */
+ * synchronous; with TC_MEM_DEVICE it is ordered on opts->stream and returns once enqueued
+ * (see the memory kinds above for when that waits). */
 TC_API int tc_decode(tc_decoder* dec, size_t n_cb, const tc_code_block* cbs, size_t llr_len,
               const float* llr, size_t post_len, float* posterior, uint8_t* crc_ok,
               uint32_t* iterations_used, const tc_decode_options* opts);
@@ -281,7 +285,8 @@ TC_API int tc_decode_transport_blocks(tc_decoder* dec, size_t n_tb, const tc_tra
  * that cannot absorb the synchronisation and latency of cudaMalloc/cudaFree, a program whose
  * device memory belongs to another allocator, a plug-in handed only its input and output
  * buffers.  No decoder object is needed; it runs on the current device, ordered on
- * opts->stream (NULL = the legacy default stream), and returns once enqueued.  llr, posterior,
+ * opts->stream (NULL = the legacy default stream), and returns once enqueued (after the work
+ * already on that stream: its descriptor copy waits for it).  llr, posterior,
  * crc_ok and iterations_used are device pointers (the last two may be NULL).
  *
  * Every other device buffer comes from a fixed 32 MiB array compiled into the library (held on
