@@ -37,6 +37,35 @@ def test_device_derate_is_bit_exact(tc, decoder):
         l_pos += 3 * (k + 4)
 
 
+def test_device_derate_covers_every_block_size(tc, decoder):
+    """Every one of the 188 block sizes, each redundancy version, fillers 0-56 and E on both
+    sides of the valid circular-buffer length (punctured and repeated): the device de-rate
+    matcher, whose circular-buffer ranks are computed in closed form per interleaver column,
+    equals the host matcher (a position walk) bit for bit."""
+    import torch
+
+    rng = np.random.default_rng(23)
+    blocks = []
+    for i, k in enumerate(e.k for e in tc.qpp_interleaver_table()):
+        for rv in range(4):
+            f = ((i + rv) % 8) * 8 if k > 64 else 0
+            e = int(rng.integers(k // 2, 3 * (k + 4))) if rv % 2 == 0 else int(rng.integers(3 * (k + 4), 7 * k))
+            blocks.append((k, f, e, rv))
+    arr, e_len, llr_len = tc.Decoder.rm_blocks(blocks)
+    x = rng.normal(0, 4, e_len).astype(np.float32)
+    xd = torch.from_numpy(x).cuda()
+    out = torch.full((llr_len,), float("nan"), device="cuda")
+    decoder.derate_device(blocks, xd.data_ptr(), e_len, out.data_ptr(), llr_len)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    e_pos = l_pos = 0
+    for k, f, e, rv in blocks:
+        ref = tc.derate_match_llr(k, f, x[e_pos:e_pos + e], rv)
+        assert np.array_equal(got[l_pos:l_pos + 3 * (k + 4)].view(np.uint32), ref.view(np.uint32)), (k, f, e, rv)
+        e_pos += e
+        l_pos += 3 * (k + 4)
+
+
 def test_transport_block_chain_matches_reference(tc, decoder, oracle):
     """Config-3 transport blocks (uneven TBS, K+/K-, filler, CRC24B, rate 0.3-0.9): the device
     chain gives the reference chain's posteriors (1e-3), decoded bits and CRC flags -- bits may
